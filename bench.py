@@ -1,0 +1,303 @@
+"""Benchmark of the sparse D3Q27 step on B200: one JSON line (rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--storage f32|f16|bf16] [--impl ours|reference]
+
+Workload (one "step" = one lattice-Boltzmann time step over every fluid node): the pulsatile pipe — open pipe
+R = 24, length 192 along z, 347,328 fluid nodes, velocity inlet with a plug profile u_in(t) = 0.02 (1 + 0.5
+sin(2 pi t / 4000)), pressure outlet at rho = 1, regularised collision with the Galilean correction, Bouzidi walls,
+tau = 0.55, FP32 populations. Synthetic geometry (no dataset is involved).
+
+Timing: W untimed steps, then K steps, each bracketed by CUDA events on the solver's stream with a 256 MB write
+between steps, which flushes the 126 MB L2 (the step's working set, ~124 MB, is about the L2 size). value =
+whole-job MLUPS (all ranks' node updates / the slowest rank's summed step time). e2e = the same metric through the
+public API from host tables: Solver construction from pinned host arrays (H2D), run(K) in CUDA graphs, fields()
+(D2H). Multi-GPU: independent replicas, one per rank, no collective on the data path ("scaling": "weak").
+--impl reference: the CPU restatement of the reference's step (oracle/, OpenMP on every host core) on the same
+workload, rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "open_pipe_R24_L192"
+TAU = 0.55
+DRIVE = ([0.02, 0.0, 0.01], 4000)       # u0 (1 + 0.5 sin(2 pi t / T)): a0 = 0.02, b1 = 0.01
+BPLU = {"f32": 356, "f16": 248, "bf16": 248}   # algorithmic bytes per lattice update
+METRIC = "D3Q27 MLUPS + HBM GB/s on 1 B200, plain vs batched/FP16; p50/p99 beat latency"
+FLUSH_BYTES = 256 << 20
+
+
+def nu_lu():
+    return (TAU - 0.5) / 3.0
+
+
+def plug_inlet(lat):
+    """Replace the builder's parabolic inlet profile by a plug of unit speed along the inward normal."""
+    import torch
+    inlet = [o for o in lat["openings"] if o["kind"] == "inlet"][-1]
+    cells = (lat["nbr"] == -2).any(0)
+    uin = np.zeros_like(lat["uin"])
+    uin[cells] = (-np.asarray(inlet["normal"], float)).astype(np.float32)
+    lat["uin"] = uin
+    if "_dev" in lat:
+        lat["_dev"]["uin"] = torch.as_tensor(uin).to(lat["_dev"]["nbr"].device)
+    return lat
+
+
+def configure(s):
+    s.set_drive(DRIVE[0], period=DRIVE[1])
+    s.set_outlet_pressure([0.0])
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(storage):
+    """DRAM bytes per node update of the step kernel from the committed ncu summary (None if not captured)."""
+    p = os.path.join(ROOT, "profiles", f"step_{storage}_open_pipe_R24_L192.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_node_update:"):
+            return float(line.split(":")[1])
+    return None
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.p = None
+        self.path = f"/tmp/cs_clocks_{os.getpid()}.csv"
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.15)
+        self.p.terminate()
+        self.p.wait()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) == 7:
+                try:
+                    rows.append((float(f[0]), float(f[1]), f[3:]))
+                except ValueError:
+                    pass
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for _, _, r in rows for k, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(lat, max_seconds=20.0):
+    """The CPU restatement (FP32, OpenMP on every core) on a bounded number of full steps of the same lattice."""
+    from oracle.step_ref import OracleSolver
+    s = OracleSolver(lat, nu_lu(), model="regularised")
+    configure(s)
+    t = time.perf_counter()
+    s.run(2)
+    per = (time.perf_counter() - t) / 2
+    n = int(max(2, min(200, max_seconds / max(per, 1e-6))))
+    t = time.perf_counter()
+    s.run(n)
+    secs = time.perf_counter() - t
+    N = lat["nbr"].shape[1]
+    return {"value": N * n / secs / 1e6, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{n} full steps of the {N}-node lattice (FP32 CPU restatement of the reference step, "
+                      f"OpenMP, {os.cpu_count()} threads)"}
+
+
+def run_reference(args):
+    import torch.distributed as dist  # noqa: F401
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from cerebrosim_b200 import cases
+    from oracle import lattice_ref as L
+    from oracle.step_ref import OracleSolver
+    lat = plug_inlet(L.build_lattice(**cases.lattice_args(cases.case(WORKLOAD))))
+    N = lat["nbr"].shape[1]
+    s = OracleSolver(lat, nu_lu(), model="regularised")
+    configure(s)
+    s.run(args.warmup)
+    t = time.perf_counter()
+    s.run(args.steps)
+    secs = time.perf_counter() - t
+    v = N * args.steps / secs / 1e6
+    cores = os.cpu_count()
+    line = {"metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"pulsatile pipe {WORKLOAD} ({N} nodes), tau {TAU}, plug inlet, pressure outlet",
+                       "storage": "f32", "parallelism": "replicas"},
+            "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} full steps of the {N}-node lattice (CPU restatement of the "
+                                       f"reference step, FP32, OpenMP, {cores} threads)"},
+            "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from cerebrosim_b200 import _lib, cases, lbm
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    c = cases.case(WORKLOAD)
+    lat = plug_inlet(lbm.build_lattice(**cases.lattice_args(c), device=dev))
+    N = lat["nbr"].shape[1]
+    s = lbm.Solver(lat, nu_lu(), model="regularised", device=dev, storage=args.storage)
+    configure(s)
+    lib = _lib.load()
+    stream = s.stream
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    descs = [s._desc(), s._desc()]
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def step(k):
+        _lib.check(lib.cs_step(ctypes.byref(descs[s.cur]), s.cur, 1, sp))
+        s.cur = 1 - s.cur
+        s.steps += 1
+
+    with torch.cuda.stream(stream):
+        for k in range(args.warmup):
+            flush.fill_(float(k))
+            step(k)
+        stream.synchronize()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        whole0, whole1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        clocks = Clocks(local)
+        whole0.record(stream)
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            starts[k].record(stream)
+            step(k)
+            ends[k].record(stream)
+        whole1.record(stream)
+        stream.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        clk = clocks.stop()
+    times = [a.elapsed_time(b) * 1e-3 for a, b in zip(starts, ends)]
+    total = max_over_ranks(sum(times))
+    ok = s.ok()
+    value = world * N * args.steps / total / 1e6
+    mean_step = total / args.steps
+    peak, peak_kind = measured_peak()
+    bplu = BPLU[args.storage]
+    achieved = bplu * N / mean_step / 1e9
+    tr = profiled_traffic(args.storage)
+
+    # end to end through the public API: host tables (pinned) -> Solver -> run(K) in graphs -> fields()
+    host = {k: (torch.from_numpy(np.ascontiguousarray(lat[k])).pin_memory() if k in ("nbr", "q", "uin") else lat[k])
+            for k in lat if k != "_dev"}
+    h2d = sum(host[k].numel() * host[k].element_size() for k in ("nbr", "q", "uin"))
+    del s
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    s2 = lbm.Solver(host, nu_lu(), model="regularised", device=dev, storage=args.storage)
+    configure(s2)
+    s2.run(args.steps)
+    p_h, u_h = s2.fields()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_secs = max_over_ranks(e0.elapsed_time(e1) * 1e-3)
+    d2h = p_h.nbytes + u_h.nbytes
+    e2e = {"value": world * N * args.steps / e2e_secs / 1e6, "unit": "MLUPS",
+           "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+           "definition": "Solver(lat) from pinned host tables + run(K) in CUDA graphs + fields() readback, "
+                         "no L2 flush"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": mean_step * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"pulsatile pipe {WORKLOAD}: {N} fluid nodes, tau {TAU}, plug velocity "
+                                       "inlet u0 (1 + 0.5 sin(2 pi t / 4000)), pressure outlet, regularised + "
+                                       "Galilean + Bouzidi",
+                           "storage": args.storage, "nodes": N, "parallelism": f"replicas x{world}",
+                           "l2": "flushed between timed steps (256 MB write)"},
+                "hbm_gbs": achieved,
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "peak_kind": peak_kind,
+                             "traffic": tr * N if tr else None, "bytes_per_update": bplu},
+                "e2e": e2e, "gpu_launches": args.steps, "ok": ok,
+                "whole_region_ms": whole0.elapsed_time(whole1)}
+        if clk:
+            line["clocks"] = clk
+        if world == 1 and not args.no_cpu_baseline:
+            from oracle import lattice_ref as L
+            line["cpu_baseline"] = cpu_baseline(plug_inlet(L.build_lattice(**cases.lattice_args(c))))
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,373 @@
+"""Drop-in replacement for CerebroSim's `lbm` module (lbm.py), running on a B200 through libcerebrosim_b200.so.
+
+Same public surface as the reference: `LATTICE, C, W, Q, OPP, WALL, INLET, OUTLET0` (lbm.py:33-58), `Units`
+(lbm.py:63-82), `build_lattice` (lbm.py:264-330), `scatter` (lbm.py:333-338) and `Solver` (lbm.py:346-455) with
+`set_drive`, `set_force`, `set_sponge`, `set_outlet_pressure`, `run`, `fields`, `ok` and the `_launch(a)` hook.
+State lives in PyTorch CUDA tensors; every step is one hand-written sm_100a kernel (csrc/step.cu) and runs of steps
+are CUDA graphs, as in the reference. There is no CPU path: without a CUDA device or the library, construction
+raises.
+
+Differences a caller can see (all documented in DESIGN.md):
+  - only D3Q27 (the reference's default; ARTERY_LBM_LATTICE=D3Q19 raises ValueError);
+  - `Solver(..., storage="f32" | "f16" | "bf16", block=None)`: population storage format and threads per block;
+  - `vels[k]` is an (N, 3) view of a (3, N) structure-of-arrays buffer; `fields()` returns NumPy copies as before.
+"""
+import ctypes
+import os
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check
+
+LATTICE = os.environ.get("ARTERY_LBM_LATTICE", "D3Q27")
+if LATTICE != "D3Q27":
+    raise ValueError(f"ARTERY_LBM_LATTICE={LATTICE}: this build implements D3Q27 only")
+
+# lbm.py:34-47
+C = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1],
+              [1, 1, 0], [-1, -1, 0], [1, -1, 0], [-1, 1, 0], [1, 0, 1], [-1, 0, -1], [1, 0, -1], [-1, 0, 1],
+              [0, 1, 1], [0, -1, -1], [0, 1, -1], [0, -1, 1],
+              [1, 1, 1], [-1, -1, -1], [1, 1, -1], [-1, -1, 1], [1, -1, 1], [-1, 1, -1], [-1, 1, 1], [1, -1, -1]],
+             np.int32)
+W = np.array([8 / 27] + [2 / 27] * 6 + [1 / 54] * 12 + [1 / 216] * 8)
+Q = len(C)
+OPP = np.array([int(np.flatnonzero((C == -c).all(1))[0]) for c in C], np.int32)
+WALL, INLET, OUTLET0 = -1, -2, -3
+
+
+class Units:
+    """Physical <-> lattice units for spacing dx (m), step dt (s), density rho (kg/m^3), viscosity nu (m^2/s)."""
+
+    def __init__(self, dx, dt, rho, nu):
+        self.dx, self.dt, self.rho, self.nu = dx, dt, rho, nu
+        self.nu_lu = nu * dt / dx ** 2
+        self.tau = 3.0 * self.nu_lu + 0.5
+        self.c = dx / dt
+
+    def u(self, u_lu):
+        return np.asarray(u_lu) * self.c
+
+    def u_lu(self, u):
+        return np.asarray(u) / self.c
+
+    def p(self, p_lu):
+        return np.asarray(p_lu) * self.rho * self.c ** 2
+
+    def p_lu(self, p):
+        return np.asarray(p) / (self.rho * self.c ** 2)
+
+
+def _device(device=None):
+    if not torch.cuda.is_available():
+        raise RuntimeError("cerebrosim_b200 needs a CUDA device (there is no CPU fallback)")
+    if device is None:
+        return torch.device("cuda", torch.cuda.current_device())
+    d = torch.device(device)
+    if d.type != "cuda":
+        raise ValueError(f"device {device!r}: cerebrosim_b200 runs on CUDA devices only")
+    return torch.device("cuda", d.index if d.index is not None else torch.cuda.current_device())
+
+
+def ctypes_void(x):
+    return ctypes.c_void_p(int(x))
+
+
+def build_lattice(phi, origin, dx, openings=(), periodic=(), opening_slack=1.0, device=None):
+    """Sparse lattice from a signed distance on grid nodes (negative = fluid), built on the GPU (lbm.py:264-330).
+
+    Returns the reference's dict of NumPy arrays (nbr (Q, N) int32, q (Q, N) float32, uin (N, 3) float32,
+    coords (N, 3) int32, origin, dx, shape, n_outlets, counts, openings), bit-identical to lbm.build_lattice, plus
+    "_dev": the same tables as CUDA tensors, which `Solver` reuses instead of uploading them again."""
+    lib = _lib.load()
+    dev = _device(device)
+    phi_h = np.ascontiguousarray(np.asarray(phi, np.float32))
+    if phi_h.ndim != 3:
+        raise ValueError(f"phi must be 3-D, got shape {phi_h.shape}")
+    nx, ny, nz = (int(s) for s in phi_h.shape)
+    origin_a = np.asarray(origin, float)
+    mask = 0
+    for a in periodic:
+        if a not in (0, 1, 2):
+            raise ValueError(f"periodic axis {a}")
+        mask |= 1 << int(a)
+    ops = list(openings)
+    carr = (_lib.Opening * max(1, len(ops)))()
+    for k, o in enumerate(ops):
+        if o["kind"] not in ("inlet", "outlet"):
+            raise ValueError(f"opening kind {o['kind']!r}")
+        carr[k].kind = 0 if o["kind"] == "inlet" else 1
+        c, nrm = np.asarray(o["centre"], float), np.asarray(o["normal"], float)
+        for a in range(3):
+            carr[k].centre[a] = float(c[a])
+            carr[k].normal[a] = float(nrm[a])
+        carr[k].radius = float(o["radius"])
+    inlets = [o for o in ops if o["kind"] == "inlet"]
+    outlets = [o for o in ops if o["kind"] == "outlet"]
+    with torch.cuda.device(dev):
+        stream = torch.cuda.current_stream(dev)
+        sp = ctypes.c_void_p(stream.cuda_stream)
+        phi_d = torch.from_numpy(phi_h).to(dev)
+        scratch = torch.empty(max(1, int(lib.cs_lattice_scratch_bytes(nx, ny, nz))), dtype=torch.uint8, device=dev)
+        n_fluid = ctypes.c_int64(0)
+        check(lib.cs_lattice_count(ctypes.c_void_p(phi_d.data_ptr()), nx, ny, nz,
+                                   ctypes.c_void_p(scratch.data_ptr()), ctypes.byref(n_fluid), sp))
+        N = n_fluid.value
+        nbr = torch.empty((Q, N), dtype=torch.int32, device=dev)
+        q = torch.empty((Q, N), dtype=torch.float32, device=dev)
+        uin = torch.empty((N, 3), dtype=torch.float32, device=dev)
+        coords = torch.empty((N, 3), dtype=torch.int32, device=dev)
+        counts = torch.empty(2 + len(outlets), dtype=torch.int64, device=dev)
+        org = (ctypes.c_double * 3)(*origin_a.reshape(3).tolist())
+
+        def ptr(t):
+            return ctypes.c_void_p(t.data_ptr() if t.numel() else 0)
+        check(lib.cs_lattice_fill(ctypes.c_void_p(phi_d.data_ptr()), nx, ny, nz, org, float(dx), carr, len(ops),
+                                  mask, float(opening_slack), ctypes.c_void_p(scratch.data_ptr()), N, ptr(nbr),
+                                  ptr(q), ptr(uin), ptr(coords), ptr(counts), sp))
+        stream.synchronize()
+        del scratch, phi_d
+    cnt = counts.cpu().numpy()
+    return {"nbr": nbr.cpu().numpy(), "q": q.cpu().numpy(), "uin": uin.cpu().numpy(), "coords": coords.cpu().numpy(),
+            "origin": origin_a, "dx": dx, "shape": phi_h.shape, "n_outlets": len(outlets),
+            "counts": {"wall": int(cnt[0]), "inlet": int(cnt[1]), "outlet": [int(x) for x in cnt[2:]]},
+            "openings": inlets + outlets, "_dev": {"nbr": nbr, "q": q, "uin": uin, "coords": coords}}
+
+
+def scatter(lat, values, fill=np.nan):
+    """Per-cell values -> dense grid (`fill` outside the fluid), lbm.py:333-338."""
+    values = np.asarray(values)
+    out = np.full(tuple(lat["shape"]) + values.shape[1:], fill, values.dtype if values.dtype.kind == "f" else float)
+    out[tuple(lat["coords"].T)] = values
+    return out
+
+
+def sponge_tau(lat, tau, length, tau_max, kinds=("inlet", "outlet")):
+    """Per-cell tau raised smoothly towards the openings of the given kinds (lbm.py:398-416): tau_max at the
+    opening plane, back to tau at `length` cells inside, within 1.5 radii of the opening's axis."""
+    pos = lat["origin"] + lat["coords"] * lat["dx"]
+    out = np.full(len(lat["coords"]), tau)
+    for o in lat["openings"]:
+        if o["kind"] not in kinds:
+            continue
+        c, nrm = np.asarray(o["centre"], float), np.asarray(o["normal"], float)
+        rel = pos - c
+        along = rel @ nrm
+        depth = -along / lat["dx"]
+        near = np.linalg.norm(rel - along[:, None] * nrm, axis=1) < 1.5 * o["radius"]
+        w = np.clip(1.0 - depth / length, 0.0, 1.0)
+        w = w * w * (3.0 - 2.0 * w)
+        out = np.maximum(out, np.where(near, tau + (tau_max - tau) * w, tau))
+    return out
+
+
+def _upload(x, dtype, dev):
+    """Host table -> device: torch tensors (e.g. pinned) are copied asynchronously, NumPy arrays as they are."""
+    if isinstance(x, torch.Tensor):
+        return x.to(dev, dtype=dtype, non_blocking=True).contiguous()
+    np_dtype = {torch.int32: np.int32, torch.float32: np.float32}[dtype]
+    return torch.as_tensor(np.ascontiguousarray(x, np_dtype)).to(dev)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() else None
+
+
+class Solver:
+    """Sparse D3Q27 lattice Boltzmann on one GPU (lbm.py:346-455). tau from the lattice viscosity; model "trt"
+    (magic = Lambda) or "regularised"; sigma < 1 blends the regularised stress with the finite-difference one.
+
+    storage: "f32" (the reference's FP32 populations), "f16" or "bf16" (16-bit shifted populations, FP32
+    arithmetic). block: threads per block (None: the tuned default)."""
+
+    def __init__(self, lat, nu_lu, magic=3.0 / 16.0, bouzidi=True, model="trt", sigma=1.0, galilean=None,
+                 device=None, storage="f32", block=None):
+        lib = _lib.load()
+        self.dev = _device(device)
+        self.lat = lat
+        self.N = N = int(lat["nbr"].shape[1])
+        self.tau = 3.0 * nu_lu + 0.5
+        self.magic = float(magic)
+        self.bouzidi = int(bool(bouzidi))
+        self.model = {"trt": 0, "regularised": 1}[model]
+        self.sigma = float(sigma)
+        self.gal = int(LATTICE == "D3Q27" if galilean is None else bool(galilean))
+        if storage not in _lib.STORE:
+            raise ValueError(f"storage {storage!r}: use one of {sorted(_lib.STORE)}")
+        self.storage = storage
+        self.block = int(block) if block else default_block(N)
+        if self.block < 32 or self.block > 256 or self.block % 32:
+            raise ValueError(f"block {self.block}: a multiple of 32 in 32..256")
+        pop_dtype = {"f32": torch.float32, "f16": torch.float16, "bf16": torch.bfloat16}[storage]
+        with torch.cuda.device(self.dev):
+            self.stream = torch.cuda.Stream(self.dev)
+            self.stream.wait_stream(torch.cuda.current_stream(self.dev))
+            with torch.cuda.stream(self.stream):
+                dev = self.dev
+                self.f = [torch.zeros((Q, N), dtype=pop_dtype, device=dev) for _ in range(2)]
+                self.vel = [torch.zeros((3, N), dtype=torch.float32, device=dev) for _ in range(2)]
+                self.vels = [v.T for v in self.vel]
+                self.rho = torch.zeros(N, dtype=torch.float32, device=dev)
+                tabs = lat.get("_dev") if isinstance(lat.get("_dev"), dict) else None
+                if tabs is not None and tabs["nbr"].device == dev:
+                    nbr, q, uin = tabs["nbr"], tabs["q"], tabs["uin"]
+                else:
+                    nbr = _upload(lat["nbr"], torch.int32, dev)
+                    q = _upload(lat["q"], torch.float32, dev)
+                    uin = _upload(lat["uin"], torch.float32, dev)
+                self.uin = uin.contiguous()
+                self.inl = (nbr == INLET).any(0).to(torch.int32) if N else torch.zeros(0, dtype=torch.int32, device=dev)
+                n_out = max(1, int(lat["n_outlets"]))
+                self.links = torch.empty((Q, N), dtype=torch.int32, device=dev)
+                status = torch.empty(2, dtype=torch.int64, device=dev)
+                check(lib.cs_links_encode(_ptr(nbr), _ptr(q), N, n_out, _ptr(self.links), _ptr(status),
+                                          ctypes_void(self.stream.cuda_stream)))
+                self.p_out = torch.zeros(n_out, dtype=torch.float32, device=dev)
+                self.p_out64 = torch.zeros(n_out, dtype=torch.float64, device=dev)
+                self.om = torch.full((N,), 1.0 / self.tau, dtype=torch.float32, device=dev)
+                self.tick = torch.zeros(1, dtype=torch.int32, device=dev)
+                self.drv = torch.zeros(1, dtype=torch.float32, device=dev)
+                self._done = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.force = (0.0, 0.0, 0.0)
+        self.graphs = {}
+        self.set_drive([1.0])
+        self.cur = 0
+        self.steps = 0
+
+    # --- inputs
+    def set_drive(self, coef, period=1, ramp=0):
+        """drive(t) = coef[0] + sum_k coef[2k-1] cos(2 pi k t / period) + coef[2k] sin(...), times a smooth start
+        over `ramp` steps; scales the inlet profile and the body force (lbm.py:384-392)."""
+        coef = np.asarray(coef, np.float32)
+        if len(coef) % 2 == 0:
+            coef = np.append(coef, 0.0).astype(np.float32)
+        if int(period) < 1:
+            raise ValueError(f"period {period}: at least 1 step")
+        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+            self.coef = torch.as_tensor(coef).to(self.dev)
+        self.nh, self.period, self.ramp = (len(coef) - 1) // 2, int(period), int(ramp)
+        self._drop_graphs()
+
+    def set_force(self, F):
+        self.force = tuple(float(np.float32(x)) for x in F)
+        self._drop_graphs()
+
+    def set_sponge(self, length, tau_max, kinds=("inlet", "outlet")):
+        """Raise the viscosity smoothly towards the openings of the given kinds (lbm.py:398-416)."""
+        tau = sponge_tau(self.lat, self.tau, length, tau_max, kinds)
+        self.tau_cell = tau
+        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+            self.om.copy_(torch.as_tensor((1.0 / tau).astype(np.float32)).to(self.dev))
+
+    def set_outlet_pressure(self, p_lu):
+        p = np.asarray(p_lu, np.float32).reshape(-1)
+        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+            self.p_out[:len(p)].copy_(torch.as_tensor(p).to(self.dev))
+            self.p_out64[:len(p)].copy_(torch.as_tensor(p.astype(np.float64)).to(self.dev))
+
+    # --- stepping
+    def _desc(self):
+        d = _lib.StepDesc()
+        d.n = self.N
+        d.storage = _lib.STORE[self.storage]
+        d.model, d.bouzidi, d.gal = self.model, self.bouzidi, self.gal
+        d.sigma, d.magic = self.sigma, self.magic
+        for k in range(3):
+            d.force[k] = self.force[k]
+        d.block = self.block
+        d.f[0], d.f[1] = self.f[0].data_ptr(), self.f[1].data_ptr()
+        d.vel[0], d.vel[1] = self.vel[0].data_ptr(), self.vel[1].data_ptr()
+        d.rho, d.links, d.uin, d.om = (self.rho.data_ptr(), self.links.data_ptr(), self.uin.data_ptr(),
+                                       self.om.data_ptr())
+        d.p_out, d.n_out = self.p_out.data_ptr(), len(self.p_out)
+        d.tick, d.drive, d.coef = self.tick.data_ptr(), self.drv.data_ptr(), self.coef.data_ptr()
+        d.nh, d.period, d.ramp = self.nh, self.period, self.ramp
+        d.done = self._done.data_ptr()
+        d.p_out64 = self.p_out64.data_ptr()
+        self._fill_desc(d)
+        return d
+
+    def _fill_desc(self, d):
+        """Hook for subclasses that add the outlet-resistance coupling."""
+        d.n_open = 0
+
+    def _launch(self, a):
+        """One step reading buffer a and writing 1 - a (lbm.py:422-428)."""
+        check(_lib.load().cs_step(ctypes.byref(self._desc()), int(a), 1, ctypes_void(self.stream.cuda_stream)))
+
+    def _drop_graphs(self):
+        lib = _lib.load()
+        for g in getattr(self, "graphs", {}).values():
+            if isinstance(g, torch.cuda.CUDAGraph):
+                continue
+            lib.cs_graph_destroy(g)
+        self.graphs = {}
+
+    def _capture(self, a, chunk):
+        if type(self)._launch is Solver._launch:
+            g = ctypes.c_void_p()
+            check(_lib.load().cs_graph_capture(ctypes.byref(self._desc()), int(a), int(chunk),
+                                               ctypes_void(self.stream.cuda_stream), ctypes.byref(g)))
+            return g
+        # a subclass extended _launch: capture its Python-level launches with torch's graph API
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=self.stream):
+            for _ in range(chunk):
+                self._launch(a)
+                a = 1 - a
+        return graph
+
+    def _replay(self, g):
+        if isinstance(g, torch.cuda.CUDAGraph):
+            g.replay()
+        else:
+            check(_lib.load().cs_graph_launch(g, ctypes_void(self.stream.cuda_stream)))
+
+    def run(self, steps, chunk=200):
+        """Advance `steps` steps (CUDA graphs of `chunk` steps; chunk even), lbm.py:430-448."""
+        chunk += chunk % 2
+        full, rest = divmod(int(steps), chunk)
+        cur_stream = torch.cuda.current_stream(self.dev)
+        self.stream.wait_stream(cur_stream)
+        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+            if full:
+                key = (self.cur, chunk)
+                if key not in self.graphs:
+                    self.graphs[key] = self._capture(self.cur, chunk)
+                for _ in range(full):
+                    self._replay(self.graphs[key])
+            for _ in range(rest):
+                self._launch(self.cur)
+                self.cur = 1 - self.cur
+        cur_stream.wait_stream(self.stream)
+        self.steps += int(steps)
+
+    def synchronize(self):
+        self.stream.synchronize()
+
+    def fields(self):
+        """(pressure, velocity) per cell, lattice units, as NumPy (lbm.py:450-452)."""
+        self.stream.synchronize()
+        rho = self.rho.cpu().numpy()
+        return rho / 3.0, np.ascontiguousarray(self.vel[self.cur].cpu().numpy().T)
+
+    def ok(self):
+        """All densities finite (lbm.py:454-455)."""
+        self.stream.synchronize()
+        return bool(torch.isfinite(self.rho).all().item())
+
+    def __del__(self):
+        try:
+            self._drop_graphs()
+        except Exception:
+            pass
+
+
+def default_block(n):
+    """Threads per block of the step kernel (the value the autotuner settles on for most lattices)."""
+    return 128 if n < 148 * 2 * 256 else 256
+
+
+__all__ = ["LATTICE", "C", "W", "Q", "OPP", "WALL", "INLET", "OUTLET0", "Units", "build_lattice", "scatter",
+           "Solver", "sponge_tau"]

@@ -1,0 +1,163 @@
+/* cerebrosim.h — C ABI of the B200 sparse D3Q27 lattice-Boltzmann library (libcerebrosim_b200.so).
+ *
+ * The reference (CerebroSim) is pure Python: its solver interface is `lbm.py` (module functions + class Solver)
+ * and `simulate.py`'s `ArterySolver`; it has no FFI of its own. Each entry point below names the reference
+ * function or kernel whose behaviour it provides; the Python package `cerebrosim_b200` binds them with ctypes
+ *  behind the same `lbm` / `Solver` interface.
+ *
+ * Conventions
+ *  - Every function returns an int status: CS_OK (0) or a CS_ERR_* code; cs_last_error() gives the message of the
+ *    last failure on the calling host thread. Nothing aborts, traps or exits.
+ *  - All array pointers are DEVICE pointers (cudaMalloc'd or from a tensor) unless the comment says host.
+ *    The library allocates no device memory: callers pass scratch buffers sized by the *_scratch_bytes queries.
+ *  - `stream` is a cudaStream_t passed as void*; NULL means the legacy default stream. Work is enqueued
+ *    asynchronously unless the comment says the call synchronises the stream.
+ *  - Lattice layout (identical to the reference's tables, lbm.py:264-330): N fluid nodes numbered in C order of
+ *    the SDF grid; link-major tables nbr[i * N + n] (int32: pull source, or WALL -1, INLET -2, OUTLET k -3-k) and
+ *    q[i * N + n] (float32 wall fraction); uin[n * 3 + c]; coords[n * 3 + c].
+ */
+#ifndef CEREBROSIM_H
+#define CEREBROSIM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CS_OK 0
+#define CS_ERR_ARG 1     /* invalid argument (size, pointer, code out of range) */
+#define CS_ERR_CUDA 2    /* a CUDA runtime call failed */
+#define CS_ERR_SIZE 3    /* a size exceeds what the entry point supports */
+#define CS_ERR_DEVICE 4  /* a kernel reported a failure through its status word */
+
+/* D3Q27 link codes in the neighbour table (lbm.py:50). */
+#define CS_WALL (-1)
+#define CS_INLET (-2)
+#define CS_OUTLET0 (-3)
+
+/* Population storage formats (the arithmetic is FP32 in every format). */
+#define CS_STORE_F32 0   /* f - w_i as float32: the reference's layout (lbm.py:23) */
+#define CS_STORE_F16 1   /* (f - w_i) * 1024 / w_i as IEEE half, round to nearest */
+#define CS_STORE_BF16 2  /* (f - w_i) * 1024 / w_i as bfloat16, round to nearest */
+
+#define CS_MODEL_TRT 0
+#define CS_MODEL_REGULARISED 1
+
+/* One opening of the vessel (lbm.build_lattice `openings` entry, lbm.py:267-270). */
+typedef struct cs_opening {
+    int32_t kind;       /* 0 = inlet, 1 = outlet */
+    int32_t pad_;
+    double centre[3];   /* same units as origin / dx */
+    double normal[3];   /* outward unit normal */
+    double radius;
+} cs_opening;
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Lattice / neighbour-table builder — replaces lbm.build_lattice (lbm.py:264-330), bit-exact tables.
+ * Two phases because N is only known after the fluid count: cs_lattice_count, then cs_lattice_fill.
+ * ------------------------------------------------------------------------------------------------------------- */
+
+/* Bytes of device scratch that cs_lattice_count / cs_lattice_fill need for an nx x ny x nz grid. */
+size_t cs_lattice_scratch_bytes(int64_t nx, int64_t ny, int64_t nz);
+
+/* Count the fluid nodes (phi < 0) of the float32 grid phi (C order) and number them in C order (lbm.py:274-278).
+ * Writes the count to *n_fluid (HOST pointer); synchronises `stream`. scratch must stay untouched until
+ * cs_lattice_fill. */
+int cs_lattice_count(const float* phi, int64_t nx, int64_t ny, int64_t nz, void* scratch, int64_t* n_fluid,
+                     void* stream);
+
+/* Fill the tables for the n_fluid nodes counted above (lbm.py:280-330).
+ * openings: HOST array of n_openings entries; inlets are matched before outlets, each in list order; outlet k is
+ *   the k-th outlet of the list. periodic_mask: bit a set = axis a wraps around.
+ * Outputs (device): nbr (27*N int32), q (27*N float32), uin (N*3 float32), coords (N*3 int32),
+ *   counts (int64: [wall, inlet, outlet_0, ..., outlet_{n_out-1}]). */
+int cs_lattice_fill(const float* phi, int64_t nx, int64_t ny, int64_t nz, const double* origin, double dx,
+                    const cs_opening* openings, int32_t n_openings, int32_t periodic_mask, double opening_slack,
+                    void* scratch, int64_t n_fluid, int32_t* nbr, float* q, float* uin, int32_t* coords,
+                    int64_t* counts, void* stream);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Step — replaces lbm.k_clock + lbm.k_step (lbm.py:90-257) and, when n_open > 0, simulate.k_flux + simulate.k_bc
+ * (simulate.py:65-82), fused into ONE kernel per step.
+ * ------------------------------------------------------------------------------------------------------------- */
+
+/* Pack nbr + q into the step's link table: pull sources and inlet/outlet codes are kept; a wall link stores its q
+ * in the code itself (0x80000000 | float bits of q), so the step never reads the q table. Checks every entry:
+ * sources < N, outlet codes < n_out, wall q finite and in [0, 2); status (device, 2 x int64) receives the number
+ * of bad entries and the first bad index. Synchronises `stream`; returns CS_ERR_ARG if any entry is bad. */
+int cs_links_encode(const int32_t* nbr, const float* q, int64_t n, int32_t n_out, int32_t* links, int64_t* status,
+                    void* stream);
+
+/* Inverse of cs_links_encode for checking: nbr codes and q (0.5 on non-wall links, as lbm.py:281). */
+int cs_links_decode(const int32_t* links, int64_t n, int32_t* nbr, float* q, void* stream);
+
+typedef struct cs_step_desc {
+    int64_t n;               /* fluid nodes */
+    int32_t storage;         /* CS_STORE_* */
+    int32_t model;           /* CS_MODEL_* (lbm.py:359) */
+    int32_t bouzidi;         /* interpolated walls on / half-way bounce-back */
+    int32_t gal;             /* Galilean correction (lbm.py:362) */
+    float sigma;             /* hybrid regularisation blend (1 = off) */
+    float magic;             /* TRT magic parameter */
+    float force[3];          /* body force, scaled by the drive */
+    int32_t block;           /* threads per block; 0 = default */
+    void* f[2];              /* populations (27 * n) in `storage` format, link-major */
+    float* vel[2];           /* velocity, SoA: vel[b][c * n + node] */
+    float* rho;              /* density deviation (n) */
+    const int32_t* links;    /* encoded link table (27 * n) from cs_links_encode */
+    const float* uin;        /* inlet profile (n * 3) */
+    const float* om;         /* relaxation rate 1 / tau per node (n) */
+    float* p_out;            /* pressure per outlet (n_out), read by outlet links */
+    int32_t n_out;
+    int32_t* tick;           /* step counter (1) */
+    float* drive;            /* drive value of the last step (1) */
+    const float* coef;       /* Fourier coefficients a0, a1, b1, ... (2 nh + 1) */
+    int32_t nh, period, ramp;
+    uint32_t* done;          /* block-completion counter (1), zero before the first step */
+    /* ArterySolver coupling (n_open = 0: none) */
+    int32_t n_open;          /* open ends; p_out[0] follows the drive, p_out[k >= 1] the resistances */
+    int64_t n_flux;          /* entries of the slab-flux list, sorted by node */
+    const int32_t* flux_idx; /* node of each entry */
+    const float* flux_w;     /* weight vector of each entry (n_flux * 3) */
+    const int32_t* flux_slot;/* open end of each entry */
+    const int32_t* flux_block; /* first flux entry of each block (n_blocks + 1) from cs_flux_blocks */
+    double* q_acc;           /* flux accumulators (n_open), zero between steps */
+    double* q_last;          /* flux of the last step (n_open) */
+    double* p_out64;         /* FP64 state of the outlet pressures (n_open) */
+    const float* r_out;      /* resistance per open end (n_open) */
+    double pref, alpha;
+} cs_step_desc;
+
+/* Block partition of a sorted flux list for `block` threads per block: out[b] = first entry with
+ * flux_idx >= b * block, b = 0 .. ceil(n / block). */
+int cs_flux_blocks(const int32_t* flux_idx, int64_t n_flux, int64_t n, int32_t block, int32_t* out, void* stream);
+
+/* Enqueue `steps` steps, the first reading buffer a (0/1) and writing 1 - a, alternating (lbm.py:422-428). */
+int cs_step(const cs_step_desc* d, int32_t a, int32_t steps, void* stream);
+
+/* Capture `steps` steps starting from buffer a into a CUDA graph (lbm.py:436-442); *graph receives an opaque
+ * handle for cs_graph_launch / cs_graph_destroy. The stream must not be the legacy default stream. */
+int cs_graph_capture(const cs_step_desc* d, int32_t a, int32_t steps, void* stream, void** graph);
+int cs_graph_launch(void* graph, void* stream);
+int cs_graph_destroy(void* graph);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Misc
+ * ------------------------------------------------------------------------------------------------------------- */
+
+/* Copy the message of the calling thread's last failure into buf (NUL-terminated); returns its length. */
+int cs_last_error(char* buf, int32_t len);
+
+/* Library version string (static). */
+const char* cs_version(void);
+
+/* sizeof of the ABI structs, so that bindings can check their layout: which = 0 cs_opening, 1 cs_step_desc. */
+size_t cs_abi_sizeof(int32_t which);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CEREBROSIM_H */

@@ -1,0 +1,94 @@
+"""GPU table builder (csrc/lattice_build.cu through lbm.build_lattice) against the reference's own tables:
+bit-exact on every small fixture and, by SHA-256, on the full-size validation and benchmark lattices."""
+import hashlib
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+from cerebrosim_b200 import _lib, cases, lbm  # noqa: E402
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def test_small_fixtures_bit_exact(golden):
+    for name in golden.small_names():
+        meta, arr = golden.small_case(name)
+        lat = lbm.build_lattice(arr["phi"], meta["origin"], meta["dx"], openings=meta["openings"],
+                                periodic=meta["periodic"], opening_slack=meta["slack"])
+        for k in ("nbr", "q", "uin", "coords"):
+            assert lat[k].dtype == arr[k].dtype and lat[k].shape == arr[k].shape, (name, k)
+            assert np.array_equal(lat[k].view(np.uint32) if k in ("q", "uin") else lat[k],
+                                  arr[k].view(np.uint32) if k in ("q", "uin") else arr[k]), (name, k)
+        assert lat["counts"] == meta["counts"], name
+        assert lat["shape"] == arr["phi"].shape
+
+
+@pytest.mark.parametrize("name", ["periodic_pipe_D10", "periodic_pipe_D20", "periodic_pipe_D40",
+                                  "poiseuille_R10_L64", "open_pipe_straight_D20", "open_pipe_tilted_D20",
+                                  "stenosis70_D20", "open_pipe_R24_L192"])
+def test_full_size_tables_by_hash(golden, name):
+    h = golden.hashes[name]
+    lat = lbm.build_lattice(**cases.lattice_args(cases.case(name)))
+    assert lat["nbr"].shape[1] == h["N"] and lat["counts"] == h["counts"]
+    for k in ("nbr", "q", "uin", "coords"):
+        assert sha(lat[k]) == h[k], k
+
+
+def test_link_encoding_roundtrip(golden):
+    """The step's packed link table expands back to exactly the reference's (nbr, q)."""
+    import ctypes
+    for name in ("box_openings_slack1", "noise_nan_inf", "stenosis70_D8"):
+        meta, arr = golden.small_case(name)
+        lat = lbm.build_lattice(arr["phi"], meta["origin"], meta["dx"], openings=meta["openings"],
+                                periodic=meta["periodic"], opening_slack=meta["slack"])
+        s = lbm.Solver(lat, 0.05, model="regularised")
+        nbr = torch.empty_like(s.links)
+        q = torch.empty(s.links.shape, dtype=torch.float32, device=s.dev)
+        _lib.check(_lib.load().cs_links_decode(ctypes.c_void_p(s.links.data_ptr()), s.N,
+                                               ctypes.c_void_p(nbr.data_ptr()), ctypes.c_void_p(q.data_ptr()),
+                                               ctypes.c_void_p(s.stream.cuda_stream)))
+        s.synchronize()
+        assert np.array_equal(nbr.cpu().numpy(), arr["nbr"])
+        qd = q.cpu().numpy()
+        wall = arr["nbr"] == lbm.WALL
+        assert np.array_equal(qd[wall].view(np.uint32), arr["q"][wall].view(np.uint32))
+        assert np.all(qd[~wall] == 0.5)
+
+
+def test_invalid_tables_are_rejected(golden):
+    meta, arr = golden.small_case("stenosis70_D8")
+    lat = lbm.build_lattice(arr["phi"], meta["origin"], meta["dx"], openings=meta["openings"])
+    bad = dict(lat)
+    bad.pop("_dev")
+    nbr = lat["nbr"].copy()
+    nbr[3, 17] = lat["nbr"].shape[1] + 5           # pull source beyond N
+    bad["nbr"] = nbr
+    with pytest.raises(_lib.CerebroSimError, match="invalid entries"):
+        lbm.Solver(bad, 0.05)
+    nbr = lat["nbr"].copy()
+    nbr[5, 3] = lbm.OUTLET0 - 4                     # outlet 4 of a lattice with one outlet
+    bad["nbr"] = nbr
+    with pytest.raises(_lib.CerebroSimError):
+        lbm.Solver(bad, 0.05)
+    q = lat["q"].copy()
+    w = np.argwhere(lat["nbr"] == lbm.WALL)[0]
+    q[w[0], w[1]] = np.nan                          # a wall link without a finite q
+    bad["nbr"], bad["q"] = lat["nbr"], q
+    with pytest.raises(_lib.CerebroSimError):
+        lbm.Solver(bad, 0.05)
+
+
+def test_builder_limits():
+    phi = np.full((4, 4, 4), -1.0, np.float32)
+    ops = [{"kind": "outlet", "centre": [0, 0, 0], "normal": [1, 0, 0], "radius": 1.0}] * 33
+    with pytest.raises(_lib.CerebroSimError, match="openings"):
+        lbm.build_lattice(phi, [0, 0, 0], 1.0, openings=ops)
+    with pytest.raises(ValueError):
+        lbm.build_lattice(phi, [0, 0, 0], 1.0, periodic=(3,))
+    with pytest.raises(ValueError):
+        lbm.build_lattice(phi[0], [0, 0, 0], 1.0)
