@@ -30,14 +30,16 @@ class Opening(ctypes.Structure):
 
 
 class StepDesc(ctypes.Structure):
-    _fields_ = [("n", ctypes.c_int64), ("storage", ctypes.c_int32), ("model", ctypes.c_int32),
+    _fields_ = [("n", ctypes.c_int64), ("npad", ctypes.c_int64), ("gmax", ctypes.c_int64),
+                ("storage", ctypes.c_int32), ("model", ctypes.c_int32),
                 ("bouzidi", ctypes.c_int32), ("gal", ctypes.c_int32), ("sigma", ctypes.c_float),
                 ("magic", ctypes.c_float), ("force", ctypes.c_float * 3), ("block", ctypes.c_int32),
                 ("f", ctypes.c_void_p * 2), ("vel", ctypes.c_void_p * 2), ("rho", ctypes.c_void_p),
-                ("links", ctypes.c_void_p), ("uin", ctypes.c_void_p), ("om", ctypes.c_void_p),
+                ("links", ctypes.c_void_p), ("gnode", ctypes.c_void_p), ("ginfo", ctypes.c_void_p),
+                ("gq", ctypes.c_void_p), ("uin", ctypes.c_void_p), ("om", ctypes.c_void_p),
                 ("p_out", ctypes.c_void_p), ("n_out", ctypes.c_int32), ("tick", ctypes.c_void_p),
                 ("drive", ctypes.c_void_p), ("coef", ctypes.c_void_p), ("nh", ctypes.c_int32),
-                ("period", ctypes.c_int32), ("ramp", ctypes.c_int32), ("done", ctypes.c_void_p),
+                ("period", ctypes.c_int32), ("ramp", ctypes.c_int32),
                 ("n_open", ctypes.c_int32), ("n_flux", ctypes.c_int64), ("flux_idx", ctypes.c_void_p),
                 ("flux_w", ctypes.c_void_p), ("flux_slot", ctypes.c_void_p), ("flux_block", ctypes.c_void_p),
                 ("q_acc", ctypes.c_void_p), ("q_last", ctypes.c_void_p), ("p_out64", ctypes.c_void_p),
@@ -53,8 +55,10 @@ SIGNATURES = {
     "cs_lattice_count": (_I32, [_P, _I64, _I64, _I64, _P, ctypes.POINTER(_I64), _P]),
     "cs_lattice_fill": (_I32, [_P, _I64, _I64, _I64, ctypes.POINTER(_D), _D, ctypes.POINTER(Opening), _I32, _I32,
                                _D, _P, _I64, _P, _P, _P, _P, _P, _P]),
-    "cs_links_encode": (_I32, [_P, _P, _I64, _I32, _P, _P, _P]),
-    "cs_links_decode": (_I32, [_P, _I64, _P, _P, _P]),
+    "cs_links_scratch_bytes": (_SZ, [_I64]),
+    "cs_links_count": (_I32, [_P, _I64, _P, ctypes.POINTER(_I64), _P]),
+    "cs_links_fill": (_I32, [_P, _P, _I64, _I32, _I64, _P, _P, _P, _P, _P, _P, _P]),
+    "cs_links_decode": (_I32, [_P, _P, _P, _I64, _I64, _P, _P, _P]),
     "cs_flux_blocks": (_I32, [_P, _I64, _I64, _I32, _P, _P]),
     "cs_step": (_I32, [ctypes.POINTER(StepDesc), _I32, _I32, _P]),
     "cs_graph_capture": (_I32, [ctypes.POINTER(StepDesc), _I32, _I32, _P, ctypes.POINTER(_P)]),

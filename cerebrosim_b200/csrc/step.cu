@@ -1,24 +1,24 @@
-// Fused sparse D3Q27 step on the GPU: the work of lbm.k_clock + lbm.k_step (lbm.py:90-257) and, for the artery
-// solver, simulate.k_flux + simulate.k_bc (simulate.py:65-82) in ONE kernel per step.
+// Sparse D3Q27 step on the GPU: lbm.k_clock + lbm.k_step (lbm.py:90-257) and, for the artery solver,
+// simulate.k_flux + simulate.k_bc (simulate.py:65-82).
 //
-// One thread per fluid node, C-ordered nodes, link-major populations f[i * N + n] (the reference's SoA layout):
-// for every link the warp's 32 pull sources are mostly consecutive, so each gathered load and each store is a
-// coalesced 128-byte line. Per node the kernel reads 27 link codes, 27 populations, omega and the previous
-// velocity (plus six neighbour velocity components for the Galilean correction, mostly L2 hits) and writes 27
-// populations, the velocity and the density: the 356 B/update of an FP32 step.
-//
-//  - clock (lbm.py:94-101): every block evaluates drive(tick) itself; the last block to finish advances tick and
-//    stores the drive value, so no separate launch is needed.
-//  - boundary links (lbm.py:156-182): wall links carry their q in the link code, so no q table is read; inlet and
-//    outlet links use uin / p_out; a cell with an inlet link is an equilibrium inlet cell (lbm.py:205-216, 370).
-//  - regularised collision (lbm.py:217-240): instead of holding 27 populations and summing c c^T (f - feq) link
-//    by link, the pull loop accumulates dr, j and Pi = sum c c^T f on the fly; by the D3Q27 isotropy
-//    sum_i w_i c c^T feq2_i = dr/3 I + u u^T, so P = Pi - dr/3 I - u u^T, which is the reference's P up to
-//    rounding. Populations are therefore streamed, not kept in registers.
-//  - TRT (lbm.py:241-255) keeps the 27 populations (it needs f_i and f_opp(i)); it is off the validated path.
-//  - slab flux + outlet resistances (simulate.py:65-82): blocks holding flux cells reduce u . w in FP64 from
-//    shared memory and add to q_acc; the last block applies k_bc in FP64 (p_out64 holds the state) and resets
-//    q_acc.
+// One step = up to three kernels on one stream:
+//  1. k_boundary — the wall / inlet / outlet link list (lbm.py:163-181). One thread per ghost slot (a boundary link
+//     of one direction); it evaluates what the reference's pull produces for that link — Bouzidi interpolation
+//     (q < 0.5 with the second node, q >= 0.5 with the node's own population), half-way bounce-back, the velocity
+//     inlet with the drive, the pressure outlet with p_out and the previous velocity — and stores it in the ghost
+//     slot f_in[i * npad + n + g] of the step's input buffer.
+//  2. k_bulk — one thread per fluid node, C-ordered nodes, link-major populations (the reference's SoA layout).
+//     Every link is a plain pull f_in[i * npad + links[i * n + node]] (a fluid source or a ghost slot), so the 27
+//     loads carry no branch and issue back to back; for each link the warp's 32 sources are mostly consecutive,
+//     so each load and store moves whole 128-byte lines. The pull accumulates dr, j and Pi = sum c c^T f on the
+//     fly; by the D3Q27 isotropy sum_i w_i c c^T feq2_i = dr/3 I + u u^T, so the regularised projection
+//     P = sum c c^T (f - feq2) (lbm.py:219-223) is Pi - dr/3 I - u u^T and no population is kept in registers.
+//     Galilean correction (lbm.py:192-204) from the six axis neighbours' previous velocity (a ghost slot gives the
+//     wall's q or marks an opening); cells with an inlet link (om < 0) get the inlet equilibrium (lbm.py:205-216);
+//     TRT (lbm.py:241-255) keeps the populations. Block 0 advances the clock: tick[1 - a] = tick[a] + 1.
+//  3. k_bc (only with the resistance coupling) — one block: p_out[0] = drive, p_out[k] relaxed towards R_k Q_k -
+//     pref in FP64, Qlast = Q, Q = 0 (simulate.py:76-82). The slab flux Q_k = sum u . w itself is reduced in the
+//     bulk kernel in FP64 by the blocks that hold flux cells (simulate.py:65-69).
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -28,36 +28,43 @@ namespace cs {
 namespace {
 
 constexpr int MAX_BLOCK = 256;
+constexpr int MIN_BLOCKS = 3;   // 3 x 256 threads per SM: the register budget that keeps the pull unspilled
 constexpr int MAX_OPEN = 8;
+constexpr int B_THREADS = 256;
 constexpr float PI_F = 3.14159265358979323846f;
 
+__constant__ int k_cx[Q] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1};
+__constant__ int k_cy[Q] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1};
+__constant__ int k_cz[Q] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1};
+
 // ---- population storage -----------------------------------------------------------------------------------------
+// 32-bit element offsets: 27 * npad < 2^31 is checked on the host.
 template <int ST> struct Pop;
 
 template <> struct Pop<CS_STORE_F32> {
-    static __device__ __forceinline__ float ld(const void* b, int64_t idx, int) {
+    static __device__ __forceinline__ float ld(const void* b, uint32_t idx, float) {
         return __ldg(static_cast<const float*>(b) + idx);
     }
-    static __device__ __forceinline__ void st(void* b, int64_t idx, int, float v) { static_cast<float*>(b)[idx] = v; }
+    static __device__ __forceinline__ void st(void* b, uint32_t idx, float, float v) { static_cast<float*>(b)[idx] = v; }
 };
 
-// 16-bit formats store (f - w_i) * 1024 / w_i: every link's values share one range, well inside FP16's normal
-// numbers, so the relative rounding error is the format's 2^-11 (FP16) or 2^-8 (BF16) at every link.
+// 16-bit formats store (f - w_i) * 1024 / w_i: all links share one range, well inside FP16's normal numbers, so the
+// relative rounding error is the format's 2^-11 (FP16) or 2^-8 (BF16) on every link. w is the link's weight.
 template <> struct Pop<CS_STORE_F16> {
-    static __device__ __forceinline__ float ld(const void* b, int64_t idx, int i) {
-        return __half2float(__ldg(static_cast<const __half*>(b) + idx)) * (wgt(i) * (1.0f / 1024.0f));
+    static __device__ __forceinline__ float ld(const void* b, uint32_t idx, float w) {
+        return __half2float(__ldg(static_cast<const __half*>(b) + idx)) * (w * (1.0f / 1024.0f));
     }
-    static __device__ __forceinline__ void st(void* b, int64_t idx, int i, float v) {
-        static_cast<__half*>(b)[idx] = __float2half_rn(v * (1024.0f / wgt(i)));
+    static __device__ __forceinline__ void st(void* b, uint32_t idx, float w, float v) {
+        static_cast<__half*>(b)[idx] = __float2half_rn(v * (1024.0f / w));
     }
 };
 
 template <> struct Pop<CS_STORE_BF16> {
-    static __device__ __forceinline__ float ld(const void* b, int64_t idx, int i) {
-        return __bfloat162float(__ldg(static_cast<const __nv_bfloat16*>(b) + idx)) * (wgt(i) * (1.0f / 1024.0f));
+    static __device__ __forceinline__ float ld(const void* b, uint32_t idx, float w) {
+        return __bfloat162float(__ldg(static_cast<const __nv_bfloat16*>(b) + idx)) * (w * (1.0f / 1024.0f));
     }
-    static __device__ __forceinline__ void st(void* b, int64_t idx, int i, float v) {
-        static_cast<__nv_bfloat16*>(b)[idx] = __float2bfloat16_rn(v * (1024.0f / wgt(i)));
+    static __device__ __forceinline__ void st(void* b, uint32_t idx, float w, float v) {
+        static_cast<__nv_bfloat16*>(b)[idx] = __float2bfloat16_rn(v * (1024.0f / w));
     }
 };
 
@@ -72,26 +79,36 @@ __device__ __forceinline__ float drive_value(const cs_step_desc& d, int t) {
     return v;
 }
 
-// One component of the non-uniform central difference (lbm.py:105-126): du_c/dx_a from the links that pull from
-// x - e_a (sm) and x + e_a (sp); a wall is u = 0 at distance max(q, 0.1), an opening u = u0 at distance 1.
-__device__ __forceinline__ float ddx(int32_t sm, int32_t sp, const float* __restrict__ comp, float u0) {
+__device__ __forceinline__ float weight_rt(int i) { return i == 0 ? 8.0f / 27.0f : (i < 7 ? 2.0f / 27.0f : (i < 19 ? 1.0f / 54.0f : 1.0f / 216.0f)); }
+
+// Non-uniform central difference (lbm.py:105-126) of one velocity component: gm / gp are the values loaded through
+// the links that pull from x - e_a (sm) and x + e_a (sp) — the neighbour's previous velocity component for a fluid
+// source, the ghost slot's gq for a boundary link (q >= 0: wall at distance max(q, 0.1) with u = 0; -1: an opening,
+// u = u0 at distance 1).
+__device__ __forceinline__ float ddx_g(int32_t sm, int32_t sp, float gm, float gp, float u0, int32_t n_nodes) {
     float h1 = 1.0f, v1 = u0, h2 = 1.0f, v2 = u0;
-    if (sm >= 0) {
-        v1 = __ldg(comp + sm);
-    } else if (is_wall(sm)) {
-        h1 = fmaxf(wall_q(sm), 0.1f);
+    if (sm < n_nodes) {
+        v1 = gm;
+    } else if (gm >= 0.0f) {
+        h1 = fmaxf(gm, 0.1f);
         v1 = 0.0f;
     }
-    if (sp >= 0) {
-        v2 = __ldg(comp + sp);
-    } else if (is_wall(sp)) {
-        h2 = fmaxf(wall_q(sp), 0.1f);
+    if (sp < n_nodes) {
+        v2 = gp;
+    } else if (gp >= 0.0f) {
+        h2 = fmaxf(gp, 0.1f);
         v2 = 0.0f;
     }
     return (h1 * h1 * (v2 - u0) + h2 * h2 * (u0 - v1)) / (h1 * h2 * (h1 + h2));
 }
 
-// Third-order equilibrium term of link i (lbm.py:129-137) from the velocity monomials m.
+// Address of what the difference along link k (1..6) reads for velocity component c: the neighbour's component, or
+// the ghost slot's q.
+__device__ __forceinline__ const float* grad_src(const cs_step_desc& d, const float* vin, int k, int c, int32_t s) {
+    return s < d.n ? vin + int64_t(c) * d.n + s : d.gq + int64_t(k) * d.gmax + (s - d.n);
+}
+
+// Third-order equilibrium term of link I (lbm.py:129-137) from the velocity monomials.
 struct Cubic {
     float xxy, xxz, xyy, yyz, xzz, yzz, xyz;
     __device__ __forceinline__ explicit Cubic(float x, float y, float z)
@@ -122,45 +139,6 @@ struct Unroll<N_, N_> {
     static __device__ __forceinline__ void run(F&&) {}
 };
 
-struct NodeCtx {
-    const cs_step_desc* d;
-    const void* fin;
-    int64_t N, n;
-    float dv;
-    float upx, upy, upz, upsq;
-};
-
-// Pull of link I when its code is not a fluid source (lbm.py:163-181).
-template <int ST, int I>
-__device__ __forceinline__ float boundary_pull(const NodeCtx& c, int32_t s, int32_t s_opp, bool& inlet_cell) {
-    constexpr int io = Lat::opp(I);
-    constexpr float w = wgt(I);
-    constexpr float cx = float(Lat::cx(I)), cy = float(Lat::cy(I)), cz = float(Lat::cz(I));
-    const float fo = Pop<ST>::ld(c.fin, int64_t(io) * c.N + c.n, io);
-    if (is_wall(s)) {
-        float v = fo;
-        if (c.d->bouzidi) {
-            const float q = wall_q(s);
-            if (q < 0.5f) {
-                if (s_opp >= 0)
-                    v = 2.0f * q * fo + (1.0f - 2.0f * q) * Pop<ST>::ld(c.fin, int64_t(io) * c.N + s_opp, io);
-            } else {
-                v = fo / (2.0f * q) + (2.0f * q - 1.0f) / (2.0f * q) * Pop<ST>::ld(c.fin, int64_t(I) * c.N + c.n, I);
-            }
-        }
-        return v;
-    }
-    if (s == CS_INLET) {
-        inlet_cell = true;
-        const float* u = c.d->uin + 3 * c.n;
-        const float cu = cx * (__ldg(u) * c.dv) + cy * (__ldg(u + 1) * c.dv) + cz * (__ldg(u + 2) * c.dv);
-        return fo + 6.0f * w * cu;
-    }
-    const int k = CS_OUTLET0 - s;
-    const float cu = cx * c.upx + cy * c.upy + cz * c.upz;
-    return -fo + 2.0f * w * (3.0f * __ldg(c.d->p_out + k) + 4.5f * cu * cu - 1.5f * c.upsq);
-}
-
 // Moment sums accumulated during the pull.
 struct Moments {
     float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
@@ -181,42 +159,88 @@ struct Moments {
     }
 };
 
+// ---- 1. boundary-link kernel --------------------------------------------------------------------------------------
+template <int ST>
+__global__ void __launch_bounds__(B_THREADS) k_boundary(const cs_step_desc d, const int a) {
+    __shared__ float s_drive;
+    if (threadIdx.x == 0) s_drive = drive_value(d, d.tick[a]);
+    __syncthreads();
+    const int i = blockIdx.y;
+    const int64_t g = int64_t(blockIdx.x) * B_THREADS + threadIdx.x;
+    if (g >= d.gmax) return;
+    const int64_t slot = int64_t(i) * d.gmax + g;
+    const int32_t node = __ldg(d.gnode + slot);
+    if (node < 0) return;                                   // padding slot of a direction with fewer links
+    const int32_t info = __ldg(d.ginfo + slot);
+    const int io = Lat::opp(i);
+    const float w = weight_rt(i), wo = weight_rt(io);
+    const uint32_t NP = uint32_t(d.npad);
+    const void* fin = d.f[a];
+    const float fo = Pop<ST>::ld(fin, uint32_t(io) * NP + uint32_t(node), wo);
+    const float cx = float(k_cx[i]), cy = float(k_cy[i]), cz = float(k_cz[i]);
+    float v;
+    if (info >= CS_WALL) {
+        // lbm.py:163-173: interpolated bounce-back, or half-way bounce-back without Bouzidi
+        v = fo;
+        if (d.bouzidi) {
+            const float q = __ldg(d.gq + slot);
+            if (q < 0.5f) {
+                if (info >= 0)
+                    v = 2.0f * q * fo + (1.0f - 2.0f * q) * Pop<ST>::ld(fin, uint32_t(io) * NP + uint32_t(info), wo);
+            } else {
+                v = fo / (2.0f * q) + (2.0f * q - 1.0f) / (2.0f * q) * Pop<ST>::ld(fin, uint32_t(i) * NP + uint32_t(node), w);
+            }
+        }
+    } else if (info == CS_INLET) {
+        // lbm.py:174-177: bounce-back with the prescribed velocity
+        const float* u = d.uin + 3 * int64_t(node);
+        const float dv = s_drive;
+        const float cu = cx * (__ldg(u) * dv) + cy * (__ldg(u + 1) * dv) + cz * (__ldg(u + 2) * dv);
+        v = fo + 6.0f * w * cu;
+    } else {
+        // lbm.py:178-181: anti-bounce-back with the outlet's pressure and the previous velocity
+        const float* vin = d.vel[a];
+        const float ux = __ldg(vin + node), uy = __ldg(vin + d.n + node), uz = __ldg(vin + 2 * d.n + node);
+        const float cu = cx * ux + cy * uy + cz * uz;
+        const float usq = ux * ux + uy * uy + uz * uz;
+        v = -fo + 2.0f * w * (3.0f * __ldg(d.p_out + (CS_OUTLET0 - info)) + 4.5f * cu * cu - 1.5f * usq);
+    }
+    Pop<ST>::st(d.f[a], uint32_t(i) * NP + uint32_t(d.n + g), w, v);
+}
+
+// ---- 2. bulk kernel -----------------------------------------------------------------------------------------------
 template <int ST, int MODEL, bool GAL>
-__device__ __forceinline__ void node_update(const cs_step_desc& d, int a, float dv, int64_t n, float& ux_o,
+__device__ __forceinline__ void node_update(const cs_step_desc& d, int a, float dv, int32_t n, float& ux_o,
                                             float& uy_o, float& uz_o) {
-    const int64_t N = d.n;
+    const int32_t N = int32_t(d.n);
+    const uint32_t NP = uint32_t(d.npad);
     const void* fin = d.f[a];
     void* fout = d.f[1 - a];
     const float* vin = d.vel[a];
     float* vout = d.vel[1 - a];
+    const int32_t* lkn = d.links + n;
 
     int32_t lk[Q];
 #pragma unroll
-    for (int i = 0; i < Q; ++i) lk[i] = __ldg(d.links + int64_t(i) * N + n);
-    const float om = __ldg(d.om + n);
-    NodeCtx c;
-    c.d = &d;
-    c.fin = fin;
-    c.N = N;
-    c.n = n;
-    c.dv = dv;
-    c.upx = __ldg(vin + n);
-    c.upy = __ldg(vin + N + n);
-    c.upz = __ldg(vin + 2 * N + n);
-    c.upsq = c.upx * c.upx + c.upy * c.upy + c.upz * c.upz;
+    for (int i = 0; i < Q; ++i) lk[i] = __ldg(lkn + int64_t(i) * N);
+    const float om_signed = __ldg(d.om + n);
+    const bool inlet_cell = om_signed < 0.0f;
+    const float om = fabsf(om_signed);
+    const float upx = __ldg(vin + n), upy = __ldg(vin + N + n), upz = __ldg(vin + 2 * N + n);
     const float Fx = d.force[0] * dv, Fy = d.force[1] * dv, Fz = d.force[2] * dv;
 
+    // six loads for the Galilean differences, issued with the pull
+    float g[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (GAL) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) g[k] = __ldg(grad_src(d, vin, 1 + k, k / 2, lk[1 + k]));
+    }
+
     Moments m;
-    bool inlet_cell = false;
     float fk[MODEL == CS_MODEL_TRT ? Q : 1];
     Unroll<0, Q>::run([&](auto ic) {
         constexpr int I = decltype(ic)::value;
-        const int32_t s = lk[I];
-        float v;
-        if (s >= 0)
-            v = Pop<ST>::ld(fin, int64_t(I) * N + s, I);
-        else
-            v = boundary_pull<ST, I>(c, s, lk[Lat::opp(I)], inlet_cell);
+        const float v = Pop<ST>::ld(fin, uint32_t(I) * NP + uint32_t(lk[I]), wgt(I));
         m.add<I>(v);
         if constexpr (MODEL == CS_MODEL_TRT) fk[I] = v;
     });
@@ -228,15 +252,15 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, float 
     if (GAL) {
         t3 = 1.0f;
         const float tp = 1.0f / om;
-        edx = 3.0f * tp * ux * ux * ddx(lk[1], lk[2], vin, c.upx);
-        edy = 3.0f * tp * uy * uy * ddx(lk[3], lk[4], vin + N, c.upy);
-        edz = 3.0f * tp * uz * uz * ddx(lk[5], lk[6], vin + 2 * N, c.upz);
+        edx = 3.0f * tp * ux * ux * ddx_g(lk[1], lk[2], g[0], g[1], upx, N);
+        edy = 3.0f * tp * uy * uy * ddx_g(lk[3], lk[4], g[2], g[3], upy, N);
+        edz = 3.0f * tp * uz * uz * ddx_g(lk[5], lk[6], g[4], g[5], upz, N);
     }
     const float dr = m.dr;
 
     if (inlet_cell) {
         // lbm.py:205-216: equilibrium at the prescribed velocity
-        const float* u = d.uin + 3 * n;
+        const float* u = d.uin + 3 * int64_t(n);
         const float tx = __ldg(u) * dv, ty = __ldg(u + 1) * dv, tz = __ldg(u + 2) * dv;
         const float tsq = tx * tx + ty * ty + tz * tz;
         const Cubic cu3(tx, ty, tz);
@@ -245,7 +269,7 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, float 
             constexpr float x = Lat::cx(I), y = Lat::cy(I), z = Lat::cz(I);
             const float cu = x * tx + y * ty + z * tz;
             const float feq = wgt(I) * (dr + 3.0f * cu + 4.5f * cu * cu - 1.5f * tsq + t3 * cu3.template h3<I>());
-            Pop<ST>::st(fout, int64_t(I) * N + n, I, feq);
+            Pop<ST>::st(fout, uint32_t(I) * NP + uint32_t(n), wgt(I), feq);
         });
         vout[n] = tx;
         vout[N + n] = ty;
@@ -259,29 +283,28 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, float 
 
     const Cubic cu3(ux, uy, uz);
     if constexpr (MODEL == CS_MODEL_REGULARISED) {
-        // P = Pi - dr/3 I - u u^T  (= sum c c^T (f - feq2), lbm.py:219-223)
         const float d3 = dr * (1.0f / 3.0f);
         float pxx = m.pxx - d3 - ux * ux, pyy = m.pyy - d3 - uy * uy, pzz = m.pzz - d3 - uz * uz;
         float pxy = m.pxy - ux * uy, pxz = m.pxz - ux * uz, pyz = m.pyz - uy * uz;
         if (d.sigma < 1.0f) {
             // hybrid regularisation (lbm.py:224-229): G[a][b] = du_b/dx_a from the previous step's velocity
-            const float* vy = vin + N;
-            const float* vz = vin + 2 * N;
-            float g[3][3];
-            const int32_t sm[3] = {lk[1], lk[3], lk[5]}, sp[3] = {lk[2], lk[4], lk[6]};
+            float gr[3][3];
+            const float u0[3] = {upx, upy, upz};
 #pragma unroll
             for (int ax = 0; ax < 3; ++ax) {
-                g[ax][0] = ddx(sm[ax], sp[ax], vin, c.upx);
-                g[ax][1] = ddx(sm[ax], sp[ax], vy, c.upy);
-                g[ax][2] = ddx(sm[ax], sp[ax], vz, c.upz);
+                const int km = 1 + 2 * ax, kp = 2 + 2 * ax;
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    gr[ax][c] = ddx_g(lk[km], lk[kp], __ldg(grad_src(d, vin, km, c, lk[km])),
+                                      __ldg(grad_src(d, vin, kp, c, lk[kp])), u0[c], N);
             }
             const float sg = d.sigma, k = (1.0f - sg) / (3.0f * om);
-            pxx = sg * pxx - k * (2.0f * g[0][0]);
-            pyy = sg * pyy - k * (2.0f * g[1][1]);
-            pzz = sg * pzz - k * (2.0f * g[2][2]);
-            pxy = sg * pxy - k * (g[0][1] + g[1][0]);
-            pxz = sg * pxz - k * (g[0][2] + g[2][0]);
-            pyz = sg * pyz - k * (g[1][2] + g[2][1]);
+            pxx = sg * pxx - k * (2.0f * gr[0][0]);
+            pyy = sg * pyy - k * (2.0f * gr[1][1]);
+            pzz = sg * pzz - k * (2.0f * gr[2][2]);
+            pxy = sg * pxy - k * (gr[0][1] + gr[1][0]);
+            pxz = sg * pxz - k * (gr[0][2] + gr[2][0]);
+            pyz = sg * pyz - k * (gr[1][2] + gr[2][1]);
         }
         pxx -= edx;
         pyy -= edy;
@@ -298,7 +321,7 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, float 
                               2.0f * (float(x * y) * pxy + float(x * z) * pxz + float(y * z) * pyz);
             const float fneq = wgt(I) * (4.5f * (cpc - trp) - 1.5f * cF);
             const float src = wgt(I) * (3.0f * cF + 9.0f * cu * cF - 3.0f * uF);
-            Pop<ST>::st(fout, int64_t(I) * N + n, I, feq + k_ne * fneq + k_src * src);
+            Pop<ST>::st(fout, uint32_t(I) * NP + uint32_t(n), wgt(I), feq + k_ne * fneq + k_src * src);
         });
     } else {
         // TRT + Guo forcing (lbm.py:241-255)
@@ -318,7 +341,7 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, float 
             const float fm = 0.5f * (fk[I] - fk[jo]);
             const float sp = wgt(I) * (9.0f * cv * cF - 3.0f * uF);
             const float smv = wgt(I) * 3.0f * cF;
-            Pop<ST>::st(fout, int64_t(I) * N + n, I,
+            Pop<ST>::st(fout, uint32_t(I) * NP + uint32_t(n), wgt(I),
                         fk[I] - om * (fp - eqp) - om_m * (fm - eqm) + (1.0f - 0.5f * om) * sp +
                             (1.0f - 0.5f * om_m) * smv + psi);
         });
@@ -333,20 +356,19 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, float 
 }
 
 template <int ST, int MODEL, bool GAL>
-__global__ void __launch_bounds__(MAX_BLOCK) k_step(const cs_step_desc d, const int a) {
+__global__ void __launch_bounds__(MAX_BLOCK, MIN_BLOCKS) k_bulk(const cs_step_desc d, const int a) {
     __shared__ float s_drive;
     __shared__ int s_tick;
-    __shared__ int s_last;
     __shared__ float s_u[3][MAX_BLOCK];
     __shared__ double s_q[MAX_OPEN];
     if (threadIdx.x == 0) {
-        s_tick = *d.tick;
+        s_tick = d.tick[a];
         s_drive = drive_value(d, s_tick);
     }
     __syncthreads();
     const float dv = s_drive;
-    const int64_t n0 = int64_t(blockIdx.x) * blockDim.x;
-    const int64_t n = n0 + threadIdx.x;
+    const int32_t n0 = int32_t(blockIdx.x) * int32_t(blockDim.x);
+    const int32_t n = n0 + int32_t(threadIdx.x);
     float ux = 0.f, uy = 0.f, uz = 0.f;
     if (n < d.n) node_update<ST, MODEL, GAL>(d, a, dv, n, ux, uy, uz);
 
@@ -360,7 +382,7 @@ __global__ void __launch_bounds__(MAX_BLOCK) k_step(const cs_step_desc d, const 
             if (threadIdx.x < MAX_OPEN) s_q[threadIdx.x] = 0.0;
             __syncthreads();
             for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-                const int loc = int(__ldg(d.flux_idx + e) - n0);
+                const int loc = __ldg(d.flux_idx + e) - n0;
                 if (loc < 0 || loc >= int(blockDim.x)) continue;  // partition built for another block size
                 const float* w = d.flux_w + 3 * int64_t(e);
                 const double v = double(s_u[0][loc]) * double(__ldg(w)) + double(s_u[1][loc]) * double(__ldg(w + 1)) +
@@ -371,47 +393,42 @@ __global__ void __launch_bounds__(MAX_BLOCK) k_step(const cs_step_desc d, const 
             if (threadIdx.x < d.n_open && s_q[threadIdx.x] != 0.0) atomicAdd(d.q_acc + threadIdx.x, s_q[threadIdx.x]);
         }
     }
-
-    // completion: the last block advances the clock (lbm.py:101-102) and applies k_bc (simulate.py:76-82)
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned prev = atomicAdd(d.done, 1u);
-        s_last = prev == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (s_last && threadIdx.x == 0) {
-        __threadfence();
-        *d.tick = s_tick + 1;
+    // the clock (lbm.py:101-102): nothing in this step reads tick[1 - a]
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        d.tick[1 - a] = s_tick + 1;
         *d.drive = dv;
-        if (d.n_open > 0) {
-            d.p_out[0] = dv;
-            d.p_out64[0] = double(dv);
-            for (int k = 0; k < d.n_open; ++k) {
-                const double qk = __ldcg(d.q_acc + k);
-                d.q_last[k] = qk;
-                if (k > 0) {
-                    const double p = d.p_out64[k] + d.alpha * (double(d.r_out[k]) * qk - d.pref - d.p_out64[k]);
-                    d.p_out64[k] = p;
-                    d.p_out[k] = float(p);
-                }
-                d.q_acc[k] = 0.0;
-            }
-        }
-        __threadfence();
-        *d.done = 0u;
     }
 }
 
-using StepFn = void (*)(const cs_step_desc, const int);
+// ---- 3. outlet resistances ----------------------------------------------------------------------------------------
+__global__ void k_bc(const cs_step_desc d) {
+    // simulate.py:76-82 in FP64; the drive of this step was stored by the bulk kernel
+    const int k = threadIdx.x;
+    if (k >= d.n_open) return;
+    const double qk = d.q_acc[k];
+    d.q_last[k] = qk;
+    if (k == 0) {
+        const float dv = *d.drive;
+        d.p_out[0] = dv;
+        d.p_out64[0] = double(dv);
+    } else {
+        const double p = d.p_out64[k] + d.alpha * (double(d.r_out[k]) * qk - d.pref - d.p_out64[k]);
+        d.p_out64[k] = p;
+        d.p_out[k] = float(p);
+    }
+    d.q_acc[k] = 0.0;
+}
+
+using BulkFn = void (*)(const cs_step_desc, const int);
+using BoundFn = void (*)(const cs_step_desc, const int);
 
 template <int ST>
-StepFn pick_model(int model, int gal) {
-    if (model == CS_MODEL_REGULARISED) return gal ? k_step<ST, CS_MODEL_REGULARISED, true> : k_step<ST, CS_MODEL_REGULARISED, false>;
-    return gal ? k_step<ST, CS_MODEL_TRT, true> : k_step<ST, CS_MODEL_TRT, false>;
+BulkFn pick_model(int model, int gal) {
+    if (model == CS_MODEL_REGULARISED) return gal ? k_bulk<ST, CS_MODEL_REGULARISED, true> : k_bulk<ST, CS_MODEL_REGULARISED, false>;
+    return gal ? k_bulk<ST, CS_MODEL_TRT, true> : k_bulk<ST, CS_MODEL_TRT, false>;
 }
 
-StepFn pick(const cs_step_desc& d) {
+BulkFn pick_bulk(const cs_step_desc& d) {
     switch (d.storage) {
         case CS_STORE_F16: return pick_model<CS_STORE_F16>(d.model, d.gal);
         case CS_STORE_BF16: return pick_model<CS_STORE_BF16>(d.model, d.gal);
@@ -419,18 +436,29 @@ StepFn pick(const cs_step_desc& d) {
     }
 }
 
+BoundFn pick_boundary(const cs_step_desc& d) {
+    switch (d.storage) {
+        case CS_STORE_F16: return k_boundary<CS_STORE_F16>;
+        case CS_STORE_BF16: return k_boundary<CS_STORE_BF16>;
+        default: return k_boundary<CS_STORE_F32>;
+    }
+}
+
 int validate(const cs_step_desc* d) {
     if (!d) return fail(CS_ERR_ARG, "cs_step: null descriptor");
     if (d->n < 0 || d->n >= (int64_t(1) << 30)) return fail(CS_ERR_SIZE, "cs_step: n = %lld", (long long)d->n);
+    if (d->gmax < 0 || d->npad != d->n + d->gmax || int64_t(Q) * d->npad >= (int64_t(1) << 31))
+        return fail(CS_ERR_SIZE, "cs_step: npad %lld must be n + gmax with 27 * npad < 2^31", (long long)d->npad);
     if (d->storage < 0 || d->storage > 2) return fail(CS_ERR_ARG, "cs_step: storage %d", d->storage);
     if (d->model != CS_MODEL_TRT && d->model != CS_MODEL_REGULARISED) return fail(CS_ERR_ARG, "cs_step: model %d", d->model);
     if (d->block != 0 && (d->block < 32 || d->block > MAX_BLOCK || d->block % 32))
         return fail(CS_ERR_ARG, "cs_step: block %d (32..%d, multiple of 32)", d->block, MAX_BLOCK);
     if (d->period < 1 || d->nh < 0 || d->ramp < 0) return fail(CS_ERR_ARG, "cs_step: period %d nh %d ramp %d", d->period, d->nh, d->ramp);
-    if (!d->tick || !d->drive || !d->coef || !d->done || !d->p_out || d->n_out < 1)
+    if (!d->tick || !d->drive || !d->coef || !d->p_out || d->n_out < 1)
         return fail(CS_ERR_ARG, "cs_step: null clock / outlet state");
     if (d->n > 0 && (!d->f[0] || !d->f[1] || !d->vel[0] || !d->vel[1] || !d->rho || !d->links || !d->uin || !d->om))
         return fail(CS_ERR_ARG, "cs_step: null lattice buffer");
+    if (d->gmax > 0 && (!d->gnode || !d->ginfo || !d->gq)) return fail(CS_ERR_ARG, "cs_step: null ghost table");
     if (d->n_open < 0 || d->n_open > MAX_OPEN || d->n_open > d->n_out)
         return fail(CS_ERR_ARG, "cs_step: n_open %d (at most %d and at most n_out %d)", d->n_open, MAX_OPEN, d->n_out);
     if (d->n_open > 0 && (!d->flux_block || !d->q_acc || !d->q_last || !d->p_out64 || !d->r_out ||
@@ -440,61 +468,29 @@ int validate(const cs_step_desc* d) {
 }
 
 int launch_steps(const cs_step_desc* d, int a, int steps, cudaStream_t st) {
-    const int block = d->block ? d->block : 256;
+    const int block = d->block ? d->block : MAX_BLOCK;
     const unsigned grid = unsigned(d->n > 0 ? ceil_div(d->n, block) : 1);
-    StepFn fn = pick(*d);
+    const dim3 bgrid(unsigned(ceil_div(d->gmax, B_THREADS)), Q);
+    BulkFn bulk = pick_bulk(*d);
+    BoundFn bound = pick_boundary(*d);
     for (int s = 0; s < steps; ++s) {
-        fn<<<grid, block, 0, st>>>(*d, a);
-        CS_CHECK_LAUNCH("k_step");
+        if (d->gmax > 0) {
+            bound<<<bgrid, B_THREADS, 0, st>>>(*d, a);
+            CS_CHECK_LAUNCH("k_boundary");
+        }
+        bulk<<<grid, block, 0, st>>>(*d, a);
+        CS_CHECK_LAUNCH("k_bulk");
+        if (d->n_open > 0) {
+            k_bc<<<1, 32, 0, st>>>(*d);
+            CS_CHECK_LAUNCH("k_bc");
+        }
         a = 1 - a;
     }
     return CS_OK;
 }
 
-// ---- link table packing -------------------------------------------------------------------------------------------
-__global__ void k_links_encode(const int32_t* __restrict__ nbr, const float* __restrict__ q, int64_t n, int n_out,
-                               int32_t* __restrict__ links, unsigned long long* __restrict__ status) {
-    const int64_t total = n * Q;
-    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
-        const int32_t s = nbr[t];
-        int32_t out = s;
-        bool bad = false;
-        if (s >= 0) {
-            bad = s >= n;
-        } else if (s == CS_WALL) {
-            const float qq = q[t];
-            const int32_t bits = __float_as_int(qq);
-            bad = !(qq >= 0.0f && qq < 2.0f);      // -0.0 passes and is stored as +0.0
-            out = int32_t(0x80000000u | uint32_t(bits & 0x3fffffff));
-        } else if (s != CS_INLET) {
-            bad = (CS_OUTLET0 - s) >= n_out;
-        }
-        if (bad) {
-            out = CS_WALL;
-            atomicAdd(status, 1ull);
-            atomicMin(status + 1, (unsigned long long)t);
-        }
-        links[t] = out;
-    }
-}
-
-__global__ void k_links_decode(const int32_t* __restrict__ links, int64_t n, int32_t* __restrict__ nbr,
-                               float* __restrict__ q) {
-    const int64_t total = n * Q;
-    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
-        const int32_t s = links[t];
-        if (is_wall(s)) {
-            nbr[t] = CS_WALL;
-            q[t] = wall_q(s);
-        } else {
-            nbr[t] = s;
-            q[t] = 0.5f;
-        }
-    }
-}
-
-__global__ void k_flux_blocks(const int32_t* __restrict__ idx, int64_t n_flux, int64_t n, int block,
-                              int32_t* __restrict__ out, int64_t n_blocks) {
+__global__ void k_flux_blocks(const int32_t* __restrict__ idx, int64_t n_flux, int block, int32_t* __restrict__ out,
+                              int64_t n_blocks) {
     const int64_t b = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
     if (b > n_blocks) return;
     const int64_t key = b * block;
@@ -511,46 +507,12 @@ __global__ void k_flux_blocks(const int32_t* __restrict__ idx, int64_t n_flux, i
 
 using namespace cs;
 
-extern "C" int cs_links_encode(const int32_t* nbr, const float* q, int64_t n, int32_t n_out, int32_t* links,
-                               int64_t* status, void* stream) {
-    if (n < 0 || n >= (int64_t(1) << 30)) return fail(CS_ERR_SIZE, "cs_links_encode: n = %lld", (long long)n);
-    if (n_out < 1) return fail(CS_ERR_ARG, "cs_links_encode: n_out %d", n_out);
-    if (n == 0) return CS_OK;
-    if (!nbr || !q || !links || !status) return fail(CS_ERR_ARG, "cs_links_encode: null buffer");
-    cudaStream_t st = as_stream(stream);
-    unsigned long long init[2] = {0ull, ~0ull};
-    CS_CUDA(cudaMemcpyAsync(status, init, sizeof(init), cudaMemcpyHostToDevice, st));
-    const unsigned grid = unsigned(std::min<int64_t>(ceil_div(n * Q, 256), 148 * 32));
-    k_links_encode<<<grid, 256, 0, st>>>(nbr, q, n, n_out, links, reinterpret_cast<unsigned long long*>(status));
-    CS_CHECK_LAUNCH("k_links_encode");
-    unsigned long long res[2];
-    CS_CUDA(cudaMemcpyAsync(res, status, sizeof(res), cudaMemcpyDeviceToHost, st));
-    CS_CUDA(cudaStreamSynchronize(st));
-    if (res[0]) {
-        const long long t = (long long)res[1];
-        return fail(CS_ERR_ARG, "cs_links_encode: %llu invalid entries; first at link %lld node %lld "
-                    "(sources must be < N, outlet codes < n_out = %d, wall q finite in [0, 2))",
-                    res[0], t / n, t % n, n_out);
-    }
-    return CS_OK;
-}
-
-extern "C" int cs_links_decode(const int32_t* links, int64_t n, int32_t* nbr, float* q, void* stream) {
-    if (n < 0) return fail(CS_ERR_ARG, "cs_links_decode: n = %lld", (long long)n);
-    if (n == 0) return CS_OK;
-    if (!links || !nbr || !q) return fail(CS_ERR_ARG, "cs_links_decode: null buffer");
-    const unsigned grid = unsigned(std::min<int64_t>(ceil_div(n * Q, 256), 148 * 32));
-    k_links_decode<<<grid, 256, 0, as_stream(stream)>>>(links, n, nbr, q);
-    CS_CHECK_LAUNCH("k_links_decode");
-    return CS_OK;
-}
-
 extern "C" int cs_flux_blocks(const int32_t* flux_idx, int64_t n_flux, int64_t n, int32_t block, int32_t* out,
                               void* stream) {
     if (n < 0 || n_flux < 0 || block < 32 || block > MAX_BLOCK || !out || (n_flux > 0 && !flux_idx))
         return fail(CS_ERR_ARG, "cs_flux_blocks: bad arguments");
     const int64_t nb = n > 0 ? ceil_div(n, block) : 1;
-    k_flux_blocks<<<unsigned(ceil_div(nb + 1, 256)), 256, 0, as_stream(stream)>>>(flux_idx, n_flux, n, block, out, nb);
+    k_flux_blocks<<<unsigned(ceil_div(nb + 1, 256)), 256, 0, as_stream(stream)>>>(flux_idx, n_flux, block, out, nb);
     CS_CHECK_LAUNCH("k_flux_blocks");
     return CS_OK;
 }

@@ -203,12 +203,9 @@ class Solver:
         with torch.cuda.device(self.dev):
             self.stream = torch.cuda.Stream(self.dev)
             self.stream.wait_stream(torch.cuda.current_stream(self.dev))
+            sp = ctypes_void(self.stream.cuda_stream)
             with torch.cuda.stream(self.stream):
                 dev = self.dev
-                self.f = [torch.zeros((Q, N), dtype=pop_dtype, device=dev) for _ in range(2)]
-                self.vel = [torch.zeros((3, N), dtype=torch.float32, device=dev) for _ in range(2)]
-                self.vels = [v.T for v in self.vel]
-                self.rho = torch.zeros(N, dtype=torch.float32, device=dev)
                 tabs = lat.get("_dev") if isinstance(lat.get("_dev"), dict) else None
                 if tabs is not None and tabs["nbr"].device == dev:
                     nbr, q, uin = tabs["nbr"], tabs["q"], tabs["uin"]
@@ -219,16 +216,33 @@ class Solver:
                 self.uin = uin.contiguous()
                 self.inl = (nbr == INLET).any(0).to(torch.int32) if N else torch.zeros(0, dtype=torch.int32, device=dev)
                 n_out = max(1, int(lat["n_outlets"]))
+                # step link tables: fluid pull sources, and a ghost slot per boundary link (csrc/links.cu)
+                scratch = torch.empty(max(1, int(lib.cs_links_scratch_bytes(N))), dtype=torch.uint8, device=dev)
+                ghosts = (ctypes.c_int64 * Q)()
+                check(lib.cs_links_count(_ptr(nbr), N, _ptr(scratch), ghosts, sp))
+                self.ghosts = [int(x) for x in ghosts]
+                self.gmax = max(self.ghosts) if N else 0
+                self.npad = N + self.gmax
+                gcols = max(1, self.gmax)
                 self.links = torch.empty((Q, N), dtype=torch.int32, device=dev)
+                self.gnode = torch.full((Q, gcols), -1, dtype=torch.int32, device=dev)
+                self.ginfo = torch.full((Q, gcols), WALL, dtype=torch.int32, device=dev)
+                self.gq = torch.full((Q, gcols), -1.0, dtype=torch.float32, device=dev)
                 status = torch.empty(2, dtype=torch.int64, device=dev)
-                check(lib.cs_links_encode(_ptr(nbr), _ptr(q), N, n_out, _ptr(self.links), _ptr(status),
-                                          ctypes_void(self.stream.cuda_stream)))
+                check(lib.cs_links_fill(_ptr(nbr), _ptr(q), N, n_out, self.gmax, _ptr(scratch), _ptr(self.links),
+                                        _ptr(self.gnode), _ptr(self.ginfo), _ptr(self.gq), _ptr(status), sp))
+                del scratch
+                self.f = [torch.zeros((Q, self.npad), dtype=pop_dtype, device=dev) for _ in range(2)]
+                self.vel = [torch.zeros((3, N), dtype=torch.float32, device=dev) for _ in range(2)]
+                self.vels = [v.T for v in self.vel]
+                self.rho = torch.zeros(N, dtype=torch.float32, device=dev)
                 self.p_out = torch.zeros(n_out, dtype=torch.float32, device=dev)
                 self.p_out64 = torch.zeros(n_out, dtype=torch.float64, device=dev)
-                self.om = torch.full((N,), 1.0 / self.tau, dtype=torch.float32, device=dev)
-                self.tick = torch.zeros(1, dtype=torch.int32, device=dev)
+                # 1 / tau per node, negated on cells with an inlet link (the kernel's inlet-cell flag)
+                self._om_sign = 1.0 - 2.0 * self.inl.to(torch.float32)
+                self.om = torch.full((N,), 1.0 / self.tau, dtype=torch.float32, device=dev) * self._om_sign
+                self.tick = torch.zeros(2, dtype=torch.int32, device=dev)
                 self.drv = torch.zeros(1, dtype=torch.float32, device=dev)
-                self._done = torch.zeros(1, dtype=torch.int32, device=dev)
         self.force = (0.0, 0.0, 0.0)
         self.graphs = {}
         self.set_drive([1.0])
@@ -258,7 +272,7 @@ class Solver:
         tau = sponge_tau(self.lat, self.tau, length, tau_max, kinds)
         self.tau_cell = tau
         with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
-            self.om.copy_(torch.as_tensor((1.0 / tau).astype(np.float32)).to(self.dev))
+            self.om.copy_(torch.as_tensor((1.0 / tau).astype(np.float32)).to(self.dev) * self._om_sign)
 
     def set_outlet_pressure(self, p_lu):
         p = np.asarray(p_lu, np.float32).reshape(-1)
@@ -269,7 +283,8 @@ class Solver:
     # --- stepping
     def _desc(self):
         d = _lib.StepDesc()
-        d.n = self.N
+        d.n, d.npad, d.gmax = self.N, self.npad, self.gmax
+        d.gnode, d.ginfo, d.gq = self.gnode.data_ptr(), self.ginfo.data_ptr(), self.gq.data_ptr()
         d.storage = _lib.STORE[self.storage]
         d.model, d.bouzidi, d.gal = self.model, self.bouzidi, self.gal
         d.sigma, d.magic = self.sigma, self.magic
@@ -283,7 +298,6 @@ class Solver:
         d.p_out, d.n_out = self.p_out.data_ptr(), len(self.p_out)
         d.tick, d.drive, d.coef = self.tick.data_ptr(), self.drv.data_ptr(), self.coef.data_ptr()
         d.nh, d.period, d.ramp = self.nh, self.period, self.ramp
-        d.done = self._done.data_ptr()
         d.p_out64 = self.p_out64.data_ptr()
         self._fill_desc(d)
         return d
@@ -345,6 +359,11 @@ class Solver:
 
     def synchronize(self):
         self.stream.synchronize()
+
+    def tick_value(self):
+        """The device step counter (k_clock's tick): steps taken since construction."""
+        self.stream.synchronize()
+        return int(self.tick[self.cur].item())
 
     def fields(self):
         """(pressure, velocity) per cell, lattice units, as NumPy (lbm.py:450-452)."""

@@ -80,21 +80,41 @@ int cs_lattice_fill(const float* phi, int64_t nx, int64_t ny, int64_t nz, const 
 
 /* ---------------------------------------------------------------------------------------------------------------
  * Step — replaces lbm.k_clock + lbm.k_step (lbm.py:90-257) and, when n_open > 0, simulate.k_flux + simulate.k_bc
- * (simulate.py:65-82), fused into ONE kernel per step.
+ * (simulate.py:65-82).
+ *
+ * Link tables of the step. Every boundary link (wall, inlet or outlet code in nbr) of direction i is given a ghost
+ * slot g in 0 .. ghosts[i]-1, numbered in node order. The population rows are npad = n + gmax long (gmax = the
+ * largest ghosts[i]); slot g of direction i lives at f[i * npad + n + g]. Each step, the boundary-link kernel writes
+ * into every ghost slot the value the reference's k_step pulls for that link (Bouzidi wall, velocity inlet,
+ * pressure outlet: lbm.py:163-181), so the bulk kernel pulls every link from links[i * n + node] (a node < n or
+ * n + g) without a branch.
+ *   gnode[i * gmax + g]  node of the slot
+ *   ginfo[i * gmax + g]  wall: the node behind it along -c_i (nbr[opp(i)][node], the Bouzidi second node) or -1;
+ *                        inlet: -2; outlet k: -3 - k
+ *   gq[i * gmax + g]     wall: q; inlet / outlet: -1
  * ------------------------------------------------------------------------------------------------------------- */
 
-/* Pack nbr + q into the step's link table: pull sources and inlet/outlet codes are kept; a wall link stores its q
- * in the code itself (0x80000000 | float bits of q), so the step never reads the q table. Checks every entry:
- * sources < N, outlet codes < n_out, wall q finite and in [0, 2); status (device, 2 x int64) receives the number
- * of bad entries and the first bad index. Synchronises `stream`; returns CS_ERR_ARG if any entry is bad. */
-int cs_links_encode(const int32_t* nbr, const float* q, int64_t n, int32_t n_out, int32_t* links, int64_t* status,
-                    void* stream);
+/* Bytes of device scratch cs_links_count / cs_links_fill need for n nodes. */
+size_t cs_links_scratch_bytes(int64_t n);
 
-/* Inverse of cs_links_encode for checking: nbr codes and q (0.5 on non-wall links, as lbm.py:281). */
-int cs_links_decode(const int32_t* links, int64_t n, int32_t* nbr, float* q, void* stream);
+/* Count the boundary links of each direction: ghosts (HOST, 27 int64). Synchronises `stream`; scratch must stay
+ * untouched until cs_links_fill. */
+int cs_links_count(const int32_t* nbr, int64_t n, void* scratch, int64_t* ghosts, void* stream);
+
+/* Build links (27 * n) and the ghost tables (27 * gmax each) from the reference's nbr / q tables. Checks every
+ * entry: pull sources < n, outlet codes < n_out, wall q finite and >= 0; status (device, 2 x int64) receives the
+ * number of bad entries and the first bad (link * n + node). Synchronises `stream`; CS_ERR_ARG if any is bad. */
+int cs_links_fill(const int32_t* nbr, const float* q, int64_t n, int32_t n_out, int64_t gmax, void* scratch,
+                  int32_t* links, int32_t* gnode, int32_t* ginfo, float* gq, int64_t* status, void* stream);
+
+/* Inverse of cs_links_fill for checking: the reference's nbr codes and q (0.5 on non-wall links, lbm.py:281). */
+int cs_links_decode(const int32_t* links, const int32_t* ginfo, const float* gq, int64_t n, int64_t gmax,
+                    int32_t* nbr, float* q, void* stream);
 
 typedef struct cs_step_desc {
     int64_t n;               /* fluid nodes */
+    int64_t npad;            /* population row length, n + gmax; 27 * npad < 2^31 */
+    int64_t gmax;            /* ghost slots per direction */
     int32_t storage;         /* CS_STORE_* */
     int32_t model;           /* CS_MODEL_* (lbm.py:359) */
     int32_t bouzidi;         /* interpolated walls on / half-way bounce-back */
@@ -102,27 +122,29 @@ typedef struct cs_step_desc {
     float sigma;             /* hybrid regularisation blend (1 = off) */
     float magic;             /* TRT magic parameter */
     float force[3];          /* body force, scaled by the drive */
-    int32_t block;           /* threads per block; 0 = default */
-    void* f[2];              /* populations (27 * n) in `storage` format, link-major */
+    int32_t block;           /* threads per block of the bulk kernel; 0 = default */
+    void* f[2];              /* populations (27 * npad) in `storage` format, link-major */
     float* vel[2];           /* velocity, SoA: vel[b][c * n + node] */
     float* rho;              /* density deviation (n) */
-    const int32_t* links;    /* encoded link table (27 * n) from cs_links_encode */
+    const int32_t* links;    /* (27 * n) from cs_links_fill */
+    const int32_t* gnode;    /* ghost tables (27 * gmax) from cs_links_fill */
+    const int32_t* ginfo;
+    const float* gq;
     const float* uin;        /* inlet profile (n * 3) */
-    const float* om;         /* relaxation rate 1 / tau per node (n) */
+    const float* om;         /* relaxation rate 1 / tau per node (n), negated on cells with an inlet link */
     float* p_out;            /* pressure per outlet (n_out), read by outlet links */
     int32_t n_out;
-    int32_t* tick;           /* step counter (1) */
+    int32_t* tick;           /* step counters (2): tick[a] is the count of a step that reads buffer a */
     float* drive;            /* drive value of the last step (1) */
     const float* coef;       /* Fourier coefficients a0, a1, b1, ... (2 nh + 1) */
     int32_t nh, period, ramp;
-    uint32_t* done;          /* block-completion counter (1), zero before the first step */
     /* ArterySolver coupling (n_open = 0: none) */
     int32_t n_open;          /* open ends; p_out[0] follows the drive, p_out[k >= 1] the resistances */
     int64_t n_flux;          /* entries of the slab-flux list, sorted by node */
     const int32_t* flux_idx; /* node of each entry */
     const float* flux_w;     /* weight vector of each entry (n_flux * 3) */
     const int32_t* flux_slot;/* open end of each entry */
-    const int32_t* flux_block; /* first flux entry of each block (n_blocks + 1) from cs_flux_blocks */
+    const int32_t* flux_block; /* first flux entry of each bulk block (n_blocks + 1) from cs_flux_blocks */
     double* q_acc;           /* flux accumulators (n_open), zero between steps */
     double* q_last;          /* flux of the last step (n_open) */
     double* p_out64;         /* FP64 state of the outlet pressures (n_open) */
@@ -134,7 +156,8 @@ typedef struct cs_step_desc {
  * flux_idx >= b * block, b = 0 .. ceil(n / block). */
 int cs_flux_blocks(const int32_t* flux_idx, int64_t n_flux, int64_t n, int32_t block, int32_t* out, void* stream);
 
-/* Enqueue `steps` steps, the first reading buffer a (0/1) and writing 1 - a, alternating (lbm.py:422-428). */
+/* Enqueue `steps` steps, the first reading buffer a (0/1) and writing 1 - a, alternating (lbm.py:422-428). A step
+ * is the boundary-link kernel (when gmax > 0), the bulk kernel and, when n_open > 0, the one-block k_bc kernel. */
 int cs_step(const cs_step_desc* d, int32_t a, int32_t steps, void* stream);
 
 /* Capture `steps` steps starting from buffer a into a CUDA graph (lbm.py:436-442); *graph receives an opaque

@@ -40,8 +40,10 @@ def test_scratch_size_is_host_only():
 @pytest.mark.parametrize("call", [
     lambda lib: lib.cs_step(None, 0, 1, None),
     lambda lib: lib.cs_graph_launch(None, None),
-    lambda lib: lib.cs_links_encode(None, None, 10, 0, None, None, None),
-    lambda lib: lib.cs_links_encode(None, None, -1, 1, None, None, None),
+    lambda lib: lib.cs_links_fill(None, None, 10, 0, 0, None, None, None, None, None, None, None),
+    lambda lib: lib.cs_links_fill(None, None, 10, 1, 80_000_000, None, None, None, None, None, None, None),
+    lambda lib: lib.cs_links_count(None, -1, None, (ctypes.c_int64 * 27)(), None),
+    lambda lib: lib.cs_links_decode(None, None, None, -1, 0, None, None, None),
     lambda lib: lib.cs_flux_blocks(None, 0, 10, 16, None, None),
     lambda lib: lib.cs_lattice_count(None, -1, 2, 2, None, ctypes.byref(ctypes.c_int64()), None),
 ])
@@ -59,6 +61,9 @@ def test_step_desc_validation_without_gpu():
     lib = _lib.load()
     d = _lib.StepDesc()
     d.n, d.period, d.block = 100, 0, 128
+    assert lib.cs_step(ctypes.byref(d), 0, 1, None) == _lib.CS_ERR_SIZE
+    assert "npad" in _lib.last_error()
+    d.npad = 100
     assert lib.cs_step(ctypes.byref(d), 0, 1, None) == _lib.CS_ERR_ARG
     assert "period" in _lib.last_error()
     d.period, d.block = 1, 100

@@ -49,10 +49,13 @@ def test_link_encoding_roundtrip(golden):
         s = lbm.Solver(lat, 0.05, model="regularised")
         nbr = torch.empty_like(s.links)
         q = torch.empty(s.links.shape, dtype=torch.float32, device=s.dev)
-        _lib.check(_lib.load().cs_links_decode(ctypes.c_void_p(s.links.data_ptr()), s.N,
-                                               ctypes.c_void_p(nbr.data_ptr()), ctypes.c_void_p(q.data_ptr()),
-                                               ctypes.c_void_p(s.stream.cuda_stream)))
+        _lib.check(_lib.load().cs_links_decode(ctypes.c_void_p(s.links.data_ptr()),
+                                               ctypes.c_void_p(s.ginfo.data_ptr()), ctypes.c_void_p(s.gq.data_ptr()),
+                                               s.N, s.gmax, ctypes.c_void_p(nbr.data_ptr()),
+                                               ctypes.c_void_p(q.data_ptr()), ctypes.c_void_p(s.stream.cuda_stream)))
         s.synchronize()
+        assert s.ghosts == [int((arr["nbr"][i] < 0).sum()) for i in range(27)]
+        assert s.npad == s.N + max(s.ghosts)
         assert np.array_equal(nbr.cpu().numpy(), arr["nbr"])
         qd = q.cpu().numpy()
         wall = arr["nbr"] == lbm.WALL
