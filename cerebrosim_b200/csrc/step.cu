@@ -1,21 +1,25 @@
 // Sparse D3Q27 step on the GPU: lbm.k_clock + lbm.k_step (lbm.py:90-257) and, for the artery solver,
 // simulate.k_flux + simulate.k_bc (simulate.py:65-82).
 //
-// One step = up to three kernels on one stream:
-//  1. k_boundary — the wall / inlet / outlet link list (lbm.py:163-181). One thread per ghost slot (a boundary link
-//     of one direction); it evaluates what the reference's pull produces for that link — Bouzidi interpolation
-//     (q < 0.5 with the second node, q >= 0.5 with the node's own population), half-way bounce-back, the velocity
-//     inlet with the drive, the pressure outlet with p_out and the previous velocity — and stores it in the ghost
-//     slot f_in[i * npad + n + g] of the step's input buffer.
+// One step = two or three kernels on one stream:
+//  1. k_boundary — the wall / inlet / outlet link list (lbm.py:163-181) and the clock (lbm.py:94-102). One thread
+//     per ghost slot (a boundary link of one direction); it evaluates what the reference's pull produces for that
+//     link — Bouzidi interpolation (q < 0.5 with the second node, q >= 0.5 with the node's own population),
+//     half-way bounce-back, the velocity inlet with the drive, the pressure outlet with p_out and the previous
+//     velocity — and stores it in the ghost slot f_in[i * npad + n + g] of the step's input buffer. Its first
+//     thread evaluates drive(tick[a]) into *drive and advances tick[1 - a] = tick[a] + 1; nothing else in the step
+//     reads tick[1 - a], and the bulk kernel reads the drive from memory instead of recomputing it.
 //  2. k_bulk — one thread per fluid node, C-ordered nodes, link-major populations (the reference's SoA layout).
 //     Every link is a plain pull f_in[i * npad + links[i * n + node]] (a fluid source or a ghost slot), so the 27
 //     loads carry no branch and issue back to back; for each link the warp's 32 sources are mostly consecutive,
-//     so each load and store moves whole 128-byte lines. The pull accumulates dr, j and Pi = sum c c^T f on the
-//     fly; by the D3Q27 isotropy sum_i w_i c c^T feq2_i = dr/3 I + u u^T, so the regularised projection
-//     P = sum c c^T (f - feq2) (lbm.py:219-223) is Pi - dr/3 I - u u^T and no population is kept in registers.
-//     Galilean correction (lbm.py:192-204) from the six axis neighbours' previous velocity (a ghost slot gives the
-//     wall's q or marks an opening); cells with an inlet link (om < 0) get the inlet equilibrium (lbm.py:205-216);
-//     TRT (lbm.py:241-255) keeps the populations. Block 0 advances the clock: tick[1 - a] = tick[a] + 1.
+//     so each load and store moves whole 128-byte lines. Links come in pairs (i, opp(i)) with c_opp = -c_i: the
+//     pull accumulates dr, j and Pi = sum c c^T f from each pair's sum and difference, and the collision output is
+//     w_i (A + E_i +- O_i) with E even and O odd in c, so each pair's terms are evaluated once. By the D3Q27
+//     isotropy sum_i w_i c c^T feq2_i = dr/3 I + u u^T, the regularised projection P = sum c c^T (f - feq2)
+//     (lbm.py:219-223) is Pi - dr/3 I - u u^T; no population is kept in registers. Galilean correction
+//     (lbm.py:192-204) from the six axis neighbours' previous velocity (a ghost slot gives the wall's q or marks an
+//     opening); cells with an inlet link (om < 0) get the inlet equilibrium (lbm.py:205-216); TRT (lbm.py:241-255)
+//     keeps the populations.
 //  3. k_bc (only with the resistance coupling) — one block: p_out[0] = drive, p_out[k] relaxed towards R_k Q_k -
 //     pref in FP64, Qlast = Q, Q = 0 (simulate.py:76-82). The slab flux Q_k = sum u . w itself is reduced in the
 //     bulk kernel in FP64 by the blocks that hold flux cells (simulate.py:65-69).
@@ -79,13 +83,16 @@ __device__ __forceinline__ float drive_value(const cs_step_desc& d, int t) {
     return v;
 }
 
-__device__ __forceinline__ float weight_rt(int i) { return i == 0 ? 8.0f / 27.0f : (i < 7 ? 2.0f / 27.0f : (i < 19 ? 1.0f / 54.0f : 1.0f / 216.0f)); }
+__device__ __forceinline__ float weight_rt(int i) {
+    return i == 0 ? 8.0f / 27.0f : (i < 7 ? 2.0f / 27.0f : (i < 19 ? 1.0f / 54.0f : 1.0f / 216.0f));
+}
 
 // Non-uniform central difference (lbm.py:105-126) of one velocity component: gm / gp are the values loaded through
 // the links that pull from x - e_a (sm) and x + e_a (sp) — the neighbour's previous velocity component for a fluid
 // source, the ghost slot's gq for a boundary link (q >= 0: wall at distance max(q, 0.1) with u = 0; -1: an opening,
-// u = u0 at distance 1).
+// u = u0 at distance 1). Two fluid neighbours (the common case) give the central difference (v2 - v1) / 2.
 __device__ __forceinline__ float ddx_g(int32_t sm, int32_t sp, float gm, float gp, float u0, int32_t n_nodes) {
+    if (sm < n_nodes && sp < n_nodes) return 0.5f * (gp - gm);
     float h1 = 1.0f, v1 = u0, h2 = 1.0f, v2 = u0;
     if (sm < n_nodes) {
         v1 = gm;
@@ -108,7 +115,7 @@ __device__ __forceinline__ const float* grad_src(const cs_step_desc& d, const fl
     return s < d.n ? vin + int64_t(c) * d.n + s : d.gq + int64_t(k) * d.gmax + (s - d.n);
 }
 
-// Third-order equilibrium term of link I (lbm.py:129-137) from the velocity monomials.
+// Third-order equilibrium term of link I (lbm.py:129-137) from the velocity monomials; odd in c.
 struct Cubic {
     float xxy, xxz, xyy, yyz, xzz, yzz, xyz;
     __device__ __forceinline__ explicit Cubic(float x, float y, float z)
@@ -119,9 +126,15 @@ struct Cubic {
         constexpr float t = 1.0f / 3.0f;
         constexpr int x = Lat::cx(I), y = Lat::cy(I), z = Lat::cz(I);
         constexpr float ax = float(x * x) - t, ay = float(y * y) - t, az = float(z * z) - t;
-        return 13.5f * (ax * (float(y) * xxy + float(z) * xxz) + ay * (float(x) * xyy + float(z) * yyz) +
-                        az * (float(x) * xzz + float(y) * yzz)) +
-               float(27 * x * y * z) * xyz;
+        float s = 0.0f;
+        if (y) s += ax * float(y) * xxy;
+        if (z) s += ax * float(z) * xxz;
+        if (x) s += ay * float(x) * xyy;
+        if (z) s += ay * float(z) * yyz;
+        if (x) s += az * float(x) * xzz;
+        if (y) s += az * float(y) * yzz;
+        if (x && y && z) s += float(2 * x * y * z) * xyz;   // 27 x y z u_x u_y u_z = 13.5 * (2 x y z) u_x u_y u_z
+        return 13.5f * s;
     }
 };
 
@@ -139,31 +152,63 @@ struct Unroll<N_, N_> {
     static __device__ __forceinline__ void run(F&&) {}
 };
 
-// Moment sums accumulated during the pull.
+// Moment sums from pulled values; a pair (I, opp(I)) enters through its sum s and difference dd.
 struct Moments {
     float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
     float pxx = 0.f, pyy = 0.f, pzz = 0.f, pxy = 0.f, pxz = 0.f, pyz = 0.f;
     template <int I>
-    __device__ __forceinline__ void add(float v) {
+    __device__ __forceinline__ void add_pair(float v, float vo) {
         constexpr int x = Lat::cx(I), y = Lat::cy(I), z = Lat::cz(I);
-        dr += v;
-        if (x) jx += x * v;
-        if (y) jy += y * v;
-        if (z) jz += z * v;
-        if (x) pxx += v;
-        if (y) pyy += v;
-        if (z) pzz += v;
-        if (x && y) pxy += (x * y) * v;
-        if (x && z) pxz += (x * z) * v;
-        if (y && z) pyz += (y * z) * v;
+        const float s = v + vo, dd = v - vo;
+        dr += s;
+        if (x) jx += x * dd;
+        if (y) jy += y * dd;
+        if (z) jz += z * dd;
+        if (x) pxx += s;
+        if (y) pyy += s;
+        if (z) pzz += s;
+        if (x && y) pxy += (x * y) * s;
+        if (x && z) pxz += (x * z) * s;
+        if (y && z) pyz += (y * z) * s;
     }
 };
 
-// ---- 1. boundary-link kernel --------------------------------------------------------------------------------------
+// c^T M c for link I with M given by its diagonal and twice its off-diagonal entries.
+template <int I>
+__device__ __forceinline__ float quad(float mxx, float myy, float mzz, float mxy2, float mxz2, float myz2) {
+    constexpr int x = Lat::cx(I), y = Lat::cy(I), z = Lat::cz(I);
+    float s = 0.0f;
+    if (x) s += mxx;
+    if (y) s += myy;
+    if (z) s += mzz;
+    if (x && y) s += float(x * y) * mxy2;
+    if (x && z) s += float(x * z) * mxz2;
+    if (y && z) s += float(y * z) * myz2;
+    return s;
+}
+
+template <int I>
+__device__ __forceinline__ float cdot(float ax, float ay, float az) {
+    constexpr int x = Lat::cx(I), y = Lat::cy(I), z = Lat::cz(I);
+    float s = 0.0f;
+    if (x) s += float(x) * ax;
+    if (y) s += float(y) * ay;
+    if (z) s += float(z) * az;
+    return s;
+}
+
+// ---- 1. boundary-link kernel and clock ----------------------------------------------------------------------------
 template <int ST>
 __global__ void __launch_bounds__(B_THREADS) k_boundary(const cs_step_desc d, const int a) {
     __shared__ float s_drive;
-    if (threadIdx.x == 0) s_drive = drive_value(d, d.tick[a]);
+    if (threadIdx.x == 0) {
+        const int t = d.tick[a];
+        s_drive = drive_value(d, t);
+        if (blockIdx.x == 0 && blockIdx.y == 0) {
+            *d.drive = s_drive;
+            d.tick[1 - a] = t + 1;
+        }
+    }
     __syncthreads();
     const int i = blockIdx.y;
     const int64_t g = int64_t(blockIdx.x) * B_THREADS + threadIdx.x;
@@ -209,9 +254,25 @@ __global__ void __launch_bounds__(B_THREADS) k_boundary(const cs_step_desc d, co
 }
 
 // ---- 2. bulk kernel -----------------------------------------------------------------------------------------------
+// Writes the 27 outputs w_i (A + E_i + O_i) of a pair-symmetric collision: E(I) even and O(I) odd in c, so link I
+// and its opposite share both (the rest link is w_0 A).
+template <int ST, class EvenOdd>
+__device__ __forceinline__ void store_pairs(void* fout, uint32_t NP, int32_t n, float A, EvenOdd&& eo) {
+    Pop<ST>::st(fout, uint32_t(n), wgt(0), wgt(0) * A);
+    Unroll<0, 13>::run([&](auto pc) {
+        constexpr int I = 1 + 2 * decltype(pc)::value;
+        constexpr int O = Lat::opp(I);
+        float e, o;
+        eo(std::integral_constant<int, I>{}, e, o);
+        const float base = A + e;
+        Pop<ST>::st(fout, uint32_t(I) * NP + uint32_t(n), wgt(I), wgt(I) * (base + o));
+        Pop<ST>::st(fout, uint32_t(O) * NP + uint32_t(n), wgt(O), wgt(O) * (base - o));
+    });
+}
+
 template <int ST, int MODEL, bool GAL>
-__device__ __forceinline__ void node_update(const cs_step_desc& d, int a, float dv, int32_t n, float& ux_o,
-                                            float& uy_o, float& uz_o) {
+__device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_t n, float& ux_o, float& uy_o,
+                                            float& uz_o) {
     const int32_t N = int32_t(d.n);
     const uint32_t NP = uint32_t(d.npad);
     const void* fin = d.f[a];
@@ -223,11 +284,9 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, float 
     int32_t lk[Q];
 #pragma unroll
     for (int i = 0; i < Q; ++i) lk[i] = __ldg(lkn + int64_t(i) * N);
+    const float dv = __ldg(d.drive);
     const float om_signed = __ldg(d.om + n);
-    const bool inlet_cell = om_signed < 0.0f;
-    const float om = fabsf(om_signed);
     const float upx = __ldg(vin + n), upy = __ldg(vin + N + n), upz = __ldg(vin + 2 * N + n);
-    const float Fx = d.force[0] * dv, Fy = d.force[1] * dv, Fz = d.force[2] * dv;
 
     // six loads for the Galilean differences, issued with the pull
     float g[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -238,23 +297,34 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, float 
 
     Moments m;
     float fk[MODEL == CS_MODEL_TRT ? Q : 1];
-    Unroll<0, Q>::run([&](auto ic) {
-        constexpr int I = decltype(ic)::value;
+    const float v0 = Pop<ST>::ld(fin, uint32_t(lk[0]), wgt(0));
+    m.dr = v0;
+    if constexpr (MODEL == CS_MODEL_TRT) fk[0] = v0;
+    Unroll<0, 13>::run([&](auto pc) {
+        constexpr int I = 1 + 2 * decltype(pc)::value;
+        constexpr int O = Lat::opp(I);
         const float v = Pop<ST>::ld(fin, uint32_t(I) * NP + uint32_t(lk[I]), wgt(I));
-        m.add<I>(v);
-        if constexpr (MODEL == CS_MODEL_TRT) fk[I] = v;
+        const float vo = Pop<ST>::ld(fin, uint32_t(O) * NP + uint32_t(lk[O]), wgt(O));
+        m.add_pair<I>(v, vo);
+        if constexpr (MODEL == CS_MODEL_TRT) {
+            fk[I] = v;
+            fk[O] = vo;
+        }
     });
 
+    const bool inlet_cell = om_signed < 0.0f;
+    const float om = fabsf(om_signed);
+    const float Fx = d.force[0] * dv, Fy = d.force[1] * dv, Fz = d.force[2] * dv;
     const float ux = m.jx + Fx * 0.5f, uy = m.jy + Fy * 0.5f, uz = m.jz + Fz * 0.5f;
     const float usq = ux * ux + uy * uy + uz * uz;
     const float uF = ux * Fx + uy * Fy + uz * Fz;
     float t3 = 0.0f, edx = 0.0f, edy = 0.0f, edz = 0.0f;
     if (GAL) {
         t3 = 1.0f;
-        const float tp = 1.0f / om;
-        edx = 3.0f * tp * ux * ux * ddx_g(lk[1], lk[2], g[0], g[1], upx, N);
-        edy = 3.0f * tp * uy * uy * ddx_g(lk[3], lk[4], g[2], g[3], upy, N);
-        edz = 3.0f * tp * uz * uz * ddx_g(lk[5], lk[6], g[4], g[5], upz, N);
+        const float tp3 = 3.0f * __frcp_rn(om);
+        edx = tp3 * ux * ux * ddx_g(lk[1], lk[2], g[0], g[1], upx, N);
+        edy = tp3 * uy * uy * ddx_g(lk[3], lk[4], g[2], g[3], upy, N);
+        edz = tp3 * uz * uz * ddx_g(lk[5], lk[6], g[4], g[5], upz, N);
     }
     const float dr = m.dr;
 
@@ -264,12 +334,11 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, float 
         const float tx = __ldg(u) * dv, ty = __ldg(u + 1) * dv, tz = __ldg(u + 2) * dv;
         const float tsq = tx * tx + ty * ty + tz * tz;
         const Cubic cu3(tx, ty, tz);
-        Unroll<0, Q>::run([&](auto ic) {
+        store_pairs<ST>(fout, NP, n, dr - 1.5f * tsq, [&](auto ic, float& e, float& o) {
             constexpr int I = decltype(ic)::value;
-            constexpr float x = Lat::cx(I), y = Lat::cy(I), z = Lat::cz(I);
-            const float cu = x * tx + y * ty + z * tz;
-            const float feq = wgt(I) * (dr + 3.0f * cu + 4.5f * cu * cu - 1.5f * tsq + t3 * cu3.template h3<I>());
-            Pop<ST>::st(fout, uint32_t(I) * NP + uint32_t(n), wgt(I), feq);
+            const float cu = cdot<I>(tx, ty, tz);
+            e = 4.5f * cu * cu;
+            o = 3.0f * cu + t3 * cu3.template h3<I>();
         });
         vout[n] = tx;
         vout[N + n] = ty;
@@ -311,17 +380,19 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, float 
         pzz -= edz;
         const float trp = (pxx + pyy + pzz) * (1.0f / 3.0f);
         const float k_ne = 1.0f - om, k_src = 1.0f - 0.5f * om;
-        Unroll<0, Q>::run([&](auto ic) {
+        // f_out = feq + (1 - om) fneq + (1 - om/2) src (lbm.py:236-240) regrouped as w (A + E +- O)
+        const float A = dr - 1.5f * usq - 4.5f * k_ne * trp - 3.0f * k_src * uF;
+        const float s = 4.5f * k_ne;
+        const float qxx = s * pxx, qyy = s * pyy, qzz = s * pzz;
+        const float qxy = 2.0f * s * pxy, qxz = 2.0f * s * pxz, qyz = 2.0f * s * pyz;
+        const float ka = 3.0f * k_src - 1.5f * k_ne, kb = 9.0f * k_src;
+        const float fax = ka * Fx, fay = ka * Fy, faz = ka * Fz;
+        const float fbx = kb * Fx, fby = kb * Fy, fbz = kb * Fz;
+        store_pairs<ST>(fout, NP, n, A, [&](auto ic, float& e, float& o) {
             constexpr int I = decltype(ic)::value;
-            constexpr int x = Lat::cx(I), y = Lat::cy(I), z = Lat::cz(I);
-            const float cu = float(x) * ux + float(y) * uy + float(z) * uz;
-            const float cF = float(x) * Fx + float(y) * Fy + float(z) * Fz;
-            const float feq = wgt(I) * (dr + 3.0f * cu + 4.5f * cu * cu - 1.5f * usq + t3 * cu3.template h3<I>());
-            const float cpc = float(x * x) * pxx + float(y * y) * pyy + float(z * z) * pzz +
-                              2.0f * (float(x * y) * pxy + float(x * z) * pxz + float(y * z) * pyz);
-            const float fneq = wgt(I) * (4.5f * (cpc - trp) - 1.5f * cF);
-            const float src = wgt(I) * (3.0f * cF + 9.0f * cu * cF - 3.0f * uF);
-            Pop<ST>::st(fout, uint32_t(I) * NP + uint32_t(n), wgt(I), feq + k_ne * fneq + k_src * src);
+            const float cu = cdot<I>(ux, uy, uz);
+            e = cu * (4.5f * cu + cdot<I>(fbx, fby, fbz)) + quad<I>(qxx, qyy, qzz, qxy, qxz, qyz);
+            o = 3.0f * cu + cdot<I>(fax, fay, faz) + t3 * cu3.template h3<I>();
         });
     } else {
         // TRT + Guo forcing (lbm.py:241-255)
@@ -357,20 +428,12 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, float 
 
 template <int ST, int MODEL, bool GAL>
 __global__ void __launch_bounds__(MAX_BLOCK, MIN_BLOCKS) k_bulk(const cs_step_desc d, const int a) {
-    __shared__ float s_drive;
-    __shared__ int s_tick;
     __shared__ float s_u[3][MAX_BLOCK];
     __shared__ double s_q[MAX_OPEN];
-    if (threadIdx.x == 0) {
-        s_tick = d.tick[a];
-        s_drive = drive_value(d, s_tick);
-    }
-    __syncthreads();
-    const float dv = s_drive;
     const int32_t n0 = int32_t(blockIdx.x) * int32_t(blockDim.x);
     const int32_t n = n0 + int32_t(threadIdx.x);
     float ux = 0.f, uy = 0.f, uz = 0.f;
-    if (n < d.n) node_update<ST, MODEL, GAL>(d, a, dv, n, ux, uy, uz);
+    if (n < d.n) node_update<ST, MODEL, GAL>(d, a, n, ux, uy, uz);
 
     if (d.n_open > 0) {
         // slab flux Q_k += u . w over this block's flux entries (simulate.py:65-69), FP64
@@ -393,16 +456,11 @@ __global__ void __launch_bounds__(MAX_BLOCK, MIN_BLOCKS) k_bulk(const cs_step_de
             if (threadIdx.x < d.n_open && s_q[threadIdx.x] != 0.0) atomicAdd(d.q_acc + threadIdx.x, s_q[threadIdx.x]);
         }
     }
-    // the clock (lbm.py:101-102): nothing in this step reads tick[1 - a]
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        d.tick[1 - a] = s_tick + 1;
-        *d.drive = dv;
-    }
 }
 
 // ---- 3. outlet resistances ----------------------------------------------------------------------------------------
 __global__ void k_bc(const cs_step_desc d) {
-    // simulate.py:76-82 in FP64; the drive of this step was stored by the bulk kernel
+    // simulate.py:76-82 in FP64; the drive of this step was stored by the boundary kernel
     const int k = threadIdx.x;
     if (k >= d.n_open) return;
     const double qk = d.q_acc[k];
@@ -419,16 +477,15 @@ __global__ void k_bc(const cs_step_desc d) {
     d.q_acc[k] = 0.0;
 }
 
-using BulkFn = void (*)(const cs_step_desc, const int);
-using BoundFn = void (*)(const cs_step_desc, const int);
+using StepFn = void (*)(const cs_step_desc, const int);
 
 template <int ST>
-BulkFn pick_model(int model, int gal) {
+StepFn pick_model(int model, int gal) {
     if (model == CS_MODEL_REGULARISED) return gal ? k_bulk<ST, CS_MODEL_REGULARISED, true> : k_bulk<ST, CS_MODEL_REGULARISED, false>;
     return gal ? k_bulk<ST, CS_MODEL_TRT, true> : k_bulk<ST, CS_MODEL_TRT, false>;
 }
 
-BulkFn pick_bulk(const cs_step_desc& d) {
+StepFn pick_bulk(const cs_step_desc& d) {
     switch (d.storage) {
         case CS_STORE_F16: return pick_model<CS_STORE_F16>(d.model, d.gal);
         case CS_STORE_BF16: return pick_model<CS_STORE_BF16>(d.model, d.gal);
@@ -436,7 +493,7 @@ BulkFn pick_bulk(const cs_step_desc& d) {
     }
 }
 
-BoundFn pick_boundary(const cs_step_desc& d) {
+StepFn pick_boundary(const cs_step_desc& d) {
     switch (d.storage) {
         case CS_STORE_F16: return k_boundary<CS_STORE_F16>;
         case CS_STORE_BF16: return k_boundary<CS_STORE_BF16>;
@@ -469,17 +526,17 @@ int validate(const cs_step_desc* d) {
 
 int launch_steps(const cs_step_desc* d, int a, int steps, cudaStream_t st) {
     const int block = d->block ? d->block : MAX_BLOCK;
-    const unsigned grid = unsigned(d->n > 0 ? ceil_div(d->n, block) : 1);
-    const dim3 bgrid(unsigned(ceil_div(d->gmax, B_THREADS)), Q);
-    BulkFn bulk = pick_bulk(*d);
-    BoundFn bound = pick_boundary(*d);
+    const unsigned grid = unsigned(d->n > 0 ? ceil_div(d->n, block) : 0);
+    const dim3 bgrid(unsigned(std::max<int64_t>(1, ceil_div(d->gmax, B_THREADS))), Q);
+    StepFn bulk = pick_bulk(*d);
+    StepFn bound = pick_boundary(*d);
     for (int s = 0; s < steps; ++s) {
-        if (d->gmax > 0) {
-            bound<<<bgrid, B_THREADS, 0, st>>>(*d, a);
-            CS_CHECK_LAUNCH("k_boundary");
+        bound<<<bgrid, B_THREADS, 0, st>>>(*d, a);       // always: it also advances the clock
+        CS_CHECK_LAUNCH("k_boundary");
+        if (grid > 0) {
+            bulk<<<grid, block, 0, st>>>(*d, a);
+            CS_CHECK_LAUNCH("k_bulk");
         }
-        bulk<<<grid, block, 0, st>>>(*d, a);
-        CS_CHECK_LAUNCH("k_bulk");
         if (d->n_open > 0) {
             k_bc<<<1, 32, 0, st>>>(*d);
             CS_CHECK_LAUNCH("k_bc");
