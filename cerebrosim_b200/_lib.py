@@ -35,7 +35,8 @@ class StepDesc(ctypes.Structure):
                 ("bouzidi", ctypes.c_int32), ("gal", ctypes.c_int32), ("sigma", ctypes.c_float),
                 ("magic", ctypes.c_float), ("force", ctypes.c_float * 3), ("block", ctypes.c_int32),
                 ("f", ctypes.c_void_p * 2), ("vel", ctypes.c_void_p * 2), ("rho", ctypes.c_void_p),
-                ("links", ctypes.c_void_p), ("gnode", ctypes.c_void_p), ("ginfo", ctypes.c_void_p),
+                ("lcode", ctypes.c_void_p), ("segdelta", ctypes.c_void_p), ("irr", ctypes.c_void_p),
+                ("n_irr", ctypes.c_int64), ("gnode", ctypes.c_void_p), ("ginfo", ctypes.c_void_p),
                 ("gq", ctypes.c_void_p), ("uin", ctypes.c_void_p), ("om", ctypes.c_void_p),
                 ("p_out", ctypes.c_void_p), ("n_out", ctypes.c_int32), ("tick", ctypes.c_void_p),
                 ("drive", ctypes.c_void_p), ("coef", ctypes.c_void_p), ("nh", ctypes.c_int32),
@@ -59,6 +60,10 @@ SIGNATURES = {
     "cs_links_count": (_I32, [_P, _I64, _P, ctypes.POINTER(_I64), _P]),
     "cs_links_fill": (_I32, [_P, _P, _I64, _I32, _I64, _P, _P, _P, _P, _P, _P, _P]),
     "cs_links_decode": (_I32, [_P, _P, _P, _I64, _I64, _P, _P, _P]),
+    "cs_compress_scratch_bytes": (_SZ, [_I64]),
+    "cs_compress_count": (_I32, [_P, _I64, _P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P]),
+    "cs_compress_fill": (_I32, [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P]),
+    "cs_compress_expand": (_I32, [_P, _P, _P, _I64, _I64, _P, _P]),
     "cs_flux_blocks": (_I32, [_P, _I64, _I64, _I32, _P, _P]),
     "cs_step": (_I32, [ctypes.POINTER(StepDesc), _I32, _I32, _P]),
     "cs_graph_capture": (_I32, [ctypes.POINTER(StepDesc), _I32, _I32, _P, ctypes.POINTER(_P)]),

@@ -83,6 +83,13 @@ __device__ __forceinline__ float drive_value(const cs_step_desc& d, int t) {
     return v;
 }
 
+// Programmatic dependent launch (sm_90+): a kernel launched with the programmatic-serialization attribute may start
+// while the previous kernel of the stream is still running; it reads only static tables until
+// grid_dependency_wait(), which returns once that kernel has completed and its writes are visible. A kernel calls
+// launch_dependents() once the next kernel may be scheduled beside it. Both are no-ops for an ordinary launch.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
 __device__ __forceinline__ float weight_rt(int i) {
     return i == 0 ? 8.0f / 27.0f : (i < 7 ? 2.0f / 27.0f : (i < 19 ? 1.0f / 54.0f : 1.0f / 216.0f));
 }
@@ -201,6 +208,15 @@ __device__ __forceinline__ float cdot(float ax, float ay, float az) {
 template <int ST>
 __global__ void __launch_bounds__(B_THREADS) k_boundary(const cs_step_desc d, const int a) {
     __shared__ float s_drive;
+    // the ghost table is static: read it before waiting for the previous kernel of the stream
+    const int i = blockIdx.y;
+    const int64_t g = int64_t(blockIdx.x) * B_THREADS + threadIdx.x;
+    const int64_t slot = int64_t(i) * d.gmax + g;
+    const bool live = g < d.gmax;
+    const int32_t node = live ? __ldg(d.gnode + slot) : -1;
+    const int32_t info = live ? __ldg(d.ginfo + slot) : 0;
+    const float qslot = live ? __ldg(d.gq + slot) : 0.0f;
+    grid_dependency_wait();
     if (threadIdx.x == 0) {
         const int t = d.tick[a];
         s_drive = drive_value(d, t);
@@ -210,13 +226,8 @@ __global__ void __launch_bounds__(B_THREADS) k_boundary(const cs_step_desc d, co
         }
     }
     __syncthreads();
-    const int i = blockIdx.y;
-    const int64_t g = int64_t(blockIdx.x) * B_THREADS + threadIdx.x;
-    if (g >= d.gmax) return;
-    const int64_t slot = int64_t(i) * d.gmax + g;
-    const int32_t node = __ldg(d.gnode + slot);
+    launch_dependents();                                    // the bulk kernel may start its static loads
     if (node < 0) return;                                   // padding slot of a direction with fewer links
-    const int32_t info = __ldg(d.ginfo + slot);
     const int io = Lat::opp(i);
     const float w = weight_rt(i), wo = weight_rt(io);
     const uint32_t NP = uint32_t(d.npad);
@@ -228,7 +239,7 @@ __global__ void __launch_bounds__(B_THREADS) k_boundary(const cs_step_desc d, co
         // lbm.py:163-173: interpolated bounce-back, or half-way bounce-back without Bouzidi
         v = fo;
         if (d.bouzidi) {
-            const float q = __ldg(d.gq + slot);
+            const float q = qslot;
             if (q < 0.5f) {
                 if (info >= 0)
                     v = 2.0f * q * fo + (1.0f - 2.0f * q) * Pop<ST>::ld(fin, uint32_t(io) * NP + uint32_t(info), wo);
@@ -270,7 +281,7 @@ __device__ __forceinline__ void store_pairs(void* fout, uint32_t NP, int32_t n, 
     });
 }
 
-template <int ST, int MODEL, bool GAL>
+template <int ST, int MODEL, bool GAL, bool FORCE>
 __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_t n, float& ux_o, float& uy_o,
                                             float& uz_o) {
     const int32_t N = int32_t(d.n);
@@ -279,13 +290,28 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
     void* fout = d.f[1 - a];
     const float* vin = d.vel[a];
     float* vout = d.vel[1 - a];
-    const int32_t* lkn = d.links + n;
-
+    // connectivity and omega are static: load them while the boundary kernel may still be running
     int32_t lk[Q];
+    const int32_t code = __ldg(d.lcode + n);
+    if (code >= 0) {
+        // one 112-byte row, shared by the warp's nodes of a segment: seven 128-bit loads
+        const int4* sd = reinterpret_cast<const int4*>(d.segdelta + int64_t(code) * CS_SEG_STRIDE);
 #pragma unroll
-    for (int i = 0; i < Q; ++i) lk[i] = __ldg(lkn + int64_t(i) * N);
-    const float dv = __ldg(d.drive);
+        for (int k = 0; k < 7; ++k) {
+            const int4 v = __ldg(sd + k);
+            lk[4 * k] = n + v.x;
+            if (4 * k + 1 < Q) lk[4 * k + 1] = n + v.y;
+            if (4 * k + 2 < Q) lk[4 * k + 2] = n + v.z;
+            if (4 * k + 3 < Q) lk[4 * k + 3] = n + v.w;
+        }
+    } else {
+        const int32_t* ir = d.irr + (-1 - code);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) lk[i] = __ldg(ir + int64_t(i) * d.n_irr);
+    }
     const float om_signed = __ldg(d.om + n);
+    grid_dependency_wait();
+    const float dv = __ldg(d.drive);
     const float upx = __ldg(vin + n), upy = __ldg(vin + N + n), upz = __ldg(vin + 2 * N + n);
 
     // six loads for the Galilean differences, issued with the pull
@@ -314,7 +340,9 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
 
     const bool inlet_cell = om_signed < 0.0f;
     const float om = fabsf(om_signed);
-    const float Fx = d.force[0] * dv, Fy = d.force[1] * dv, Fz = d.force[2] * dv;
+    // without a body force (FORCE false) every force term folds away at compile time
+    const float Fx = FORCE ? d.force[0] * dv : 0.0f, Fy = FORCE ? d.force[1] * dv : 0.0f;
+    const float Fz = FORCE ? d.force[2] * dv : 0.0f;
     const float ux = m.jx + Fx * 0.5f, uy = m.jy + Fy * 0.5f, uz = m.jz + Fz * 0.5f;
     const float usq = ux * ux + uy * uy + uz * uz;
     const float uF = ux * Fx + uy * Fy + uz * Fz;
@@ -426,14 +454,16 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
     uz_o = uz;
 }
 
-template <int ST, int MODEL, bool GAL>
+template <int ST, int MODEL, bool GAL, bool FORCE>
 __global__ void __launch_bounds__(MAX_BLOCK, MIN_BLOCKS) k_bulk(const cs_step_desc d, const int a) {
     __shared__ float s_u[3][MAX_BLOCK];
     __shared__ double s_q[MAX_OPEN];
     const int32_t n0 = int32_t(blockIdx.x) * int32_t(blockDim.x);
     const int32_t n = n0 + int32_t(threadIdx.x);
     float ux = 0.f, uy = 0.f, uz = 0.f;
-    if (n < d.n) node_update<ST, MODEL, GAL>(d, a, n, ux, uy, uz);
+    if (n < d.n) node_update<ST, MODEL, GAL, FORCE>(d, a, n, ux, uy, uz);
+    grid_dependency_wait();      // (threads without a node) the flux accumulators were reset by the last step
+    launch_dependents();
 
     if (d.n_open > 0) {
         // slab flux Q_k += u . w over this block's flux entries (simulate.py:65-69), FP64
@@ -480,16 +510,26 @@ __global__ void k_bc(const cs_step_desc d) {
 using StepFn = void (*)(const cs_step_desc, const int);
 
 template <int ST>
-StepFn pick_model(int model, int gal) {
-    if (model == CS_MODEL_REGULARISED) return gal ? k_bulk<ST, CS_MODEL_REGULARISED, true> : k_bulk<ST, CS_MODEL_REGULARISED, false>;
-    return gal ? k_bulk<ST, CS_MODEL_TRT, true> : k_bulk<ST, CS_MODEL_TRT, false>;
+StepFn pick_force(int model, int gal, bool force) {
+    if (model == CS_MODEL_REGULARISED) {
+        if (gal) return force ? k_bulk<ST, CS_MODEL_REGULARISED, true, true> : k_bulk<ST, CS_MODEL_REGULARISED, true, false>;
+        return force ? k_bulk<ST, CS_MODEL_REGULARISED, false, true> : k_bulk<ST, CS_MODEL_REGULARISED, false, false>;
+    }
+    if (gal) return force ? k_bulk<ST, CS_MODEL_TRT, true, true> : k_bulk<ST, CS_MODEL_TRT, true, false>;
+    return force ? k_bulk<ST, CS_MODEL_TRT, false, true> : k_bulk<ST, CS_MODEL_TRT, false, false>;
+}
+
+template <int ST>
+StepFn pick_model(const cs_step_desc& d) {
+    const bool force = d.force[0] != 0.0f || d.force[1] != 0.0f || d.force[2] != 0.0f;
+    return pick_force<ST>(d.model, d.gal, force);
 }
 
 StepFn pick_bulk(const cs_step_desc& d) {
     switch (d.storage) {
-        case CS_STORE_F16: return pick_model<CS_STORE_F16>(d.model, d.gal);
-        case CS_STORE_BF16: return pick_model<CS_STORE_BF16>(d.model, d.gal);
-        default: return pick_model<CS_STORE_F32>(d.model, d.gal);
+        case CS_STORE_F16: return pick_model<CS_STORE_F16>(d);
+        case CS_STORE_BF16: return pick_model<CS_STORE_BF16>(d);
+        default: return pick_model<CS_STORE_F32>(d);
     }
 }
 
@@ -513,7 +553,7 @@ int validate(const cs_step_desc* d) {
     if (d->period < 1 || d->nh < 0 || d->ramp < 0) return fail(CS_ERR_ARG, "cs_step: period %d nh %d ramp %d", d->period, d->nh, d->ramp);
     if (!d->tick || !d->drive || !d->coef || !d->p_out || d->n_out < 1)
         return fail(CS_ERR_ARG, "cs_step: null clock / outlet state");
-    if (d->n > 0 && (!d->f[0] || !d->f[1] || !d->vel[0] || !d->vel[1] || !d->rho || !d->links || !d->uin || !d->om))
+    if (d->n > 0 && (!d->f[0] || !d->f[1] || !d->vel[0] || !d->vel[1] || !d->rho || !d->lcode || !d->uin || !d->om))
         return fail(CS_ERR_ARG, "cs_step: null lattice buffer");
     if (d->gmax > 0 && (!d->gnode || !d->ginfo || !d->gq)) return fail(CS_ERR_ARG, "cs_step: null ghost table");
     if (d->n_open < 0 || d->n_open > MAX_OPEN || d->n_open > d->n_out)
@@ -524,6 +564,23 @@ int validate(const cs_step_desc* d) {
     return CS_OK;
 }
 
+// Launch with programmatic stream serialization, so the kernel's static prologue overlaps the previous kernel.
+int launch_pdl(StepFn fn, dim3 grid, dim3 block, cudaStream_t st, const cs_step_desc& d, int a) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, fn, d, a);
+    if (e != cudaSuccess) return fail(CS_ERR_CUDA, "launch of a step kernel failed: %s", cudaGetErrorString(e));
+    return CS_OK;
+}
+
 int launch_steps(const cs_step_desc* d, int a, int steps, cudaStream_t st) {
     const int block = d->block ? d->block : MAX_BLOCK;
     const unsigned grid = unsigned(d->n > 0 ? ceil_div(d->n, block) : 0);
@@ -531,11 +588,12 @@ int launch_steps(const cs_step_desc* d, int a, int steps, cudaStream_t st) {
     StepFn bulk = pick_bulk(*d);
     StepFn bound = pick_boundary(*d);
     for (int s = 0; s < steps; ++s) {
-        bound<<<bgrid, B_THREADS, 0, st>>>(*d, a);       // always: it also advances the clock
-        CS_CHECK_LAUNCH("k_boundary");
+        // always launched: it also advances the clock
+        int rc = launch_pdl(bound, bgrid, dim3(B_THREADS), st, *d, a);
+        if (rc != CS_OK) return rc;
         if (grid > 0) {
-            bulk<<<grid, block, 0, st>>>(*d, a);
-            CS_CHECK_LAUNCH("k_bulk");
+            rc = launch_pdl(bulk, dim3(grid), dim3(block), st, *d, a);
+            if (rc != CS_OK) return rc;
         }
         if (d->n_open > 0) {
             k_bc<<<1, 32, 0, st>>>(*d);

@@ -35,6 +35,7 @@ W = np.array([8 / 27] + [2 / 27] * 6 + [1 / 54] * 12 + [1 / 216] * 8)
 Q = len(C)
 OPP = np.array([int(np.flatnonzero((C == -c).all(1))[0]) for c in C], np.int32)
 WALL, INLET, OUTLET0 = -1, -2, -3
+SEG_STRIDE = 28          # words per row of the compressed connectivity's segment table (CS_SEG_STRIDE)
 
 
 class Units:
@@ -232,6 +233,22 @@ class Solver:
                 check(lib.cs_links_fill(_ptr(nbr), _ptr(q), N, n_out, self.gmax, _ptr(scratch), _ptr(self.links),
                                         _ptr(self.gnode), _ptr(self.ginfo), _ptr(self.gq), _ptr(status), sp))
                 del scratch
+                # compressed connectivity (csrc/compress.cu): 4 bytes per regular node instead of 108
+                scratch = torch.empty(max(1, int(lib.cs_compress_scratch_bytes(N))), dtype=torch.uint8, device=dev)
+                n_seg, n_irr = ctypes.c_int64(0), ctypes.c_int64(0)
+                check(lib.cs_compress_count(_ptr(self.links), N, _ptr(scratch), ctypes.byref(n_seg),
+                                            ctypes.byref(n_irr), sp))
+                self.n_seg, self.n_irr = int(n_seg.value), int(n_irr.value)
+                self.lcode = torch.empty(max(1, N), dtype=torch.int32, device=dev)
+                self.segdelta = torch.empty((max(1, self.n_seg), SEG_STRIDE), dtype=torch.int32, device=dev)
+                self.irr = torch.empty((Q, max(1, self.n_irr)), dtype=torch.int32, device=dev)
+                assert self.segdelta.numel() >= self.n_seg * SEG_STRIDE and self.irr.numel() >= self.n_irr * Q
+                assert self.segdelta.data_ptr() % 16 == 0   # rows are read with 128-bit loads
+                check(lib.cs_compress_fill(_ptr(self.links), N, self.n_seg, self.n_irr, _ptr(scratch),
+                                           _ptr(self.lcode), _ptr(self.segdelta), _ptr(self.irr), sp))
+                self.stream.synchronize()
+                del scratch
+                self.links = None                          # the full 27 x N table is not needed by the step
                 self.f = [torch.zeros((Q, self.npad), dtype=pop_dtype, device=dev) for _ in range(2)]
                 self.vel = [torch.zeros((3, N), dtype=torch.float32, device=dev) for _ in range(2)]
                 self.vels = [v.T for v in self.vel]
@@ -293,8 +310,9 @@ class Solver:
         d.block = self.block
         d.f[0], d.f[1] = self.f[0].data_ptr(), self.f[1].data_ptr()
         d.vel[0], d.vel[1] = self.vel[0].data_ptr(), self.vel[1].data_ptr()
-        d.rho, d.links, d.uin, d.om = (self.rho.data_ptr(), self.links.data_ptr(), self.uin.data_ptr(),
-                                       self.om.data_ptr())
+        d.rho, d.uin, d.om = self.rho.data_ptr(), self.uin.data_ptr(), self.om.data_ptr()
+        d.lcode, d.segdelta, d.irr, d.n_irr = (self.lcode.data_ptr(), self.segdelta.data_ptr(), self.irr.data_ptr(),
+                                               max(1, self.n_irr))
         d.p_out, d.n_out = self.p_out.data_ptr(), len(self.p_out)
         d.tick, d.drive, d.coef = self.tick.data_ptr(), self.drv.data_ptr(), self.coef.data_ptr()
         d.nh, d.period, d.ramp = self.nh, self.period, self.ramp
@@ -359,6 +377,16 @@ class Solver:
 
     def synchronize(self):
         self.stream.synchronize()
+
+    def link_table(self):
+        """The step's 27 x N pull-source table (nodes < N, ghost slots >= N), expanded from its compressed form."""
+        links = torch.empty((Q, self.N), dtype=torch.int32, device=self.dev)
+        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+            check(_lib.load().cs_compress_expand(_ptr(self.lcode), _ptr(self.segdelta), _ptr(self.irr), self.N,
+                                                 max(1, self.n_irr), _ptr(links),
+                                                 ctypes_void(self.stream.cuda_stream)))
+        self.stream.synchronize()
+        return links
 
     def tick_value(self):
         """The device step counter (k_clock's tick): steps taken since construction."""

@@ -42,6 +42,9 @@ extern "C" {
 #define CS_STORE_F16 1   /* (f - w_i) * 1024 / w_i as IEEE half, round to nearest */
 #define CS_STORE_BF16 2  /* (f - w_i) * 1024 / w_i as bfloat16, round to nearest */
 
+/* Words per row of the segment delta table (27 deltas + 1 padding word). */
+#define CS_SEG_STRIDE 28
+
 #define CS_MODEL_TRT 0
 #define CS_MODEL_REGULARISED 1
 
@@ -111,6 +114,20 @@ int cs_links_fill(const int32_t* nbr, const float* q, int64_t n, int32_t n_out, 
 int cs_links_decode(const int32_t* links, const int32_t* ginfo, const float* gq, int64_t n, int64_t gmax,
                     int32_t* nbr, float* q, void* stream);
 
+/* Compressed pull connectivity of the bulk kernel, built from the links table of cs_links_fill. A node whose 27 codes
+ * are all fluid sources and whose deltas (code - node) equal those of the previous node shares its segment:
+ *   lcode[node] = s >= 0: sources node + segdelta[s * CS_SEG_STRIDE + i] (rows padded to 28 words, 16-byte
+ *                         aligned, so the bulk kernel reads a row with seven 128-bit loads);
+ *   lcode[node] = -1 - k: irregular node (some ghost link), codes irr[i * n_irr + k].
+ * count (synchronises `stream`; n_seg / n_irr are HOST outputs), then fill with the same scratch. */
+size_t cs_compress_scratch_bytes(int64_t n);
+int cs_compress_count(const int32_t* links, int64_t n, void* scratch, int64_t* n_seg, int64_t* n_irr, void* stream);
+int cs_compress_fill(const int32_t* links, int64_t n, int64_t n_seg, int64_t n_irr, void* scratch, int32_t* lcode,
+                     int32_t* segdelta, int32_t* irr, void* stream);
+/* Inverse, for checking: the 27 x n links table from the compressed form. */
+int cs_compress_expand(const int32_t* lcode, const int32_t* segdelta, const int32_t* irr, int64_t n, int64_t n_irr,
+                       int32_t* links, void* stream);
+
 typedef struct cs_step_desc {
     int64_t n;               /* fluid nodes */
     int64_t npad;            /* population row length, n + gmax; 27 * npad < 2^31 */
@@ -126,7 +143,10 @@ typedef struct cs_step_desc {
     void* f[2];              /* populations (27 * npad) in `storage` format, link-major */
     float* vel[2];           /* velocity, SoA: vel[b][c * n + node] */
     float* rho;              /* density deviation (n) */
-    const int32_t* links;    /* (27 * n) from cs_links_fill */
+    const int32_t* lcode;    /* compressed connectivity (n) from cs_compress_fill */
+    const int32_t* segdelta; /* (CS_SEG_STRIDE * n_seg), 16-byte aligned */
+    const int32_t* irr;      /* (27 * n_irr) */
+    int64_t n_irr;
     const int32_t* gnode;    /* ghost tables (27 * gmax) from cs_links_fill */
     const int32_t* ginfo;
     const float* gq;
@@ -176,7 +196,8 @@ int cs_last_error(char* buf, int32_t len);
 /* Library version string (static). */
 const char* cs_version(void);
 
-/* sizeof of the ABI structs, so that bindings can check their layout: which = 0 cs_opening, 1 cs_step_desc. */
+/* sizeof of the ABI structs, so that bindings can check their layout: which = 0 cs_opening, 1 cs_step_desc;
+ * which = 2 returns CS_SEG_STRIDE. */
 size_t cs_abi_sizeof(int32_t which);
 
 #ifdef __cplusplus

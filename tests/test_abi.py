@@ -27,6 +27,8 @@ def test_abi_sizes_and_version():
     assert lib.cs_abi_sizeof(0) == ctypes.sizeof(_lib.Opening) == 64
     assert lib.cs_abi_sizeof(1) == ctypes.sizeof(_lib.StepDesc)
     assert lib.cs_abi_sizeof(7) == 0
+    from cerebrosim_b200 import lbm
+    assert lib.cs_abi_sizeof(2) == lbm.SEG_STRIDE
     assert b"sm_100a" in lib.cs_version()
 
 

@@ -47,9 +47,10 @@ def test_link_encoding_roundtrip(golden):
         lat = lbm.build_lattice(arr["phi"], meta["origin"], meta["dx"], openings=meta["openings"],
                                 periodic=meta["periodic"], opening_slack=meta["slack"])
         s = lbm.Solver(lat, 0.05, model="regularised")
-        nbr = torch.empty_like(s.links)
-        q = torch.empty(s.links.shape, dtype=torch.float32, device=s.dev)
-        _lib.check(_lib.load().cs_links_decode(ctypes.c_void_p(s.links.data_ptr()),
+        links = s.link_table()                       # expanded from the compressed connectivity
+        nbr = torch.empty_like(links)
+        q = torch.empty(links.shape, dtype=torch.float32, device=s.dev)
+        _lib.check(_lib.load().cs_links_decode(ctypes.c_void_p(links.data_ptr()),
                                                ctypes.c_void_p(s.ginfo.data_ptr()), ctypes.c_void_p(s.gq.data_ptr()),
                                                s.N, s.gmax, ctypes.c_void_p(nbr.data_ptr()),
                                                ctypes.c_void_p(q.data_ptr()), ctypes.c_void_p(s.stream.cuda_stream)))
@@ -61,6 +62,22 @@ def test_link_encoding_roundtrip(golden):
         wall = arr["nbr"] == lbm.WALL
         assert np.array_equal(qd[wall].view(np.uint32), arr["q"][wall].view(np.uint32))
         assert np.all(qd[~wall] == 0.5)
+
+
+@pytest.mark.parametrize("name", ["open_pipe_R24_L192", "open_pipe_tilted_D20", "stenosis70_D20"])
+def test_compressed_connectivity(name):
+    """Regular nodes share segment delta vectors; the compressed form expands back to the full pull table."""
+    lat = lbm.build_lattice(**cases.lattice_args(cases.case(name)))
+    s = lbm.Solver(lat, 0.05, model="regularised")
+    links = s.link_table().cpu().numpy()
+    nbr = lat["nbr"]
+    fluid = nbr >= 0
+    assert np.array_equal(links[fluid], nbr[fluid])
+    assert np.all(links[~fluid] >= s.N)
+    irregular = (~fluid).any(0)
+    assert s.n_irr == int(irregular.sum())
+    assert s.n_seg < 0.05 * s.N                       # a few segments per row, not per node
+    print(name, s.N, "irregular", s.n_irr, "segments", s.n_seg)
 
 
 def test_invalid_tables_are_rejected(golden):
