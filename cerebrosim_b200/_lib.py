@@ -60,6 +60,7 @@ SIGNATURES = {
     "cs_links_count": (_I32, [_P, _I64, _P, ctypes.POINTER(_I64), _P]),
     "cs_links_fill": (_I32, [_P, _P, _I64, _I32, _I64, _P, _P, _P, _P, _P, _P, _P]),
     "cs_links_decode": (_I32, [_P, _P, _P, _I64, _I64, _P, _P, _P]),
+    "cs_links_build_noalloc": (_I32, [_P, _P, _I64, _I32, _I64, _P, _P, _P, _P, ctypes.POINTER(_I64), _P]),
     "cs_compress_scratch_bytes": (_SZ, [_I64]),
     "cs_compress_count": (_I32, [_P, _I64, _P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P]),
     "cs_compress_fill": (_I32, [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P]),

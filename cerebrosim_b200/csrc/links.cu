@@ -222,3 +222,96 @@ extern "C" int cs_links_decode(const int32_t* links, const int32_t* ginfo, const
     CS_CHECK_LAUNCH("k_links_decode");
     return CS_OK;
 }
+
+// ---- link-table build that allocates nothing --------------------------------------------------------------------
+// The scratch of cs_links_count / cs_links_fill (per-tile ghost counts and offsets, two status words) lives here, in
+// memory the library owns, instead of in a caller's buffer. Every GPU that loads the library holds this array until
+// the process exits. Every call shares it: the tile sums are rewritten and the status words reset by each call
+// before they are read, and two calls that overlap on the GPU race on it.
+namespace cs {
+namespace {
+
+constexpr int64_t NOALLOC_MAX_NODES = int64_t(1) << 24;                    // 16,777,216 fluid nodes
+constexpr int64_t NOALLOC_TILES = NOALLOC_MAX_NODES / T_NODES;              // 4,096 tiles of 4,096 nodes
+constexpr int64_t NOALLOC_WORDS = int64_t(Q) * (NOALLOC_TILES + 1) + 2;    // tile sums + status: about 885 KB
+
+static __device__ __align__(256) int64_t g_noalloc_scratch[NOALLOC_WORDS];
+
+constexpr int MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+int64_t* g_noalloc_ptr[MAX_DEVICES] = {};
+
+// Device address of the static scratch on the current device. The host-side name g_noalloc_scratch is only a
+// stand-in for the symbol, never a device address, so the address is looked up once per device (with that device
+// current) and cached.
+int noalloc_scratch(int64_t** out) {
+    int dev = 0;
+    CS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= MAX_DEVICES) return fail(CS_ERR_SIZE, "cs_links_build_noalloc: device %d", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(CS_ERR_CUDA, "cs_links_build_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = static_cast<int64_t*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return CS_OK;
+}
+
+}  // namespace
+}  // namespace cs
+
+extern "C" int cs_links_build_noalloc(const int32_t* nbr, const float* q, int64_t n, int32_t n_out,
+                                      int64_t gmax_cap, int32_t* links, int32_t* gnode, int32_t* ginfo, float* gq,
+                                      int64_t* ghosts, void* stream) {
+    if (!ghosts) return fail(CS_ERR_ARG, "cs_links_build_noalloc: null ghosts");
+    for (int i = 0; i < Q; ++i) ghosts[i] = 0;
+    if (n < 0 || n > NOALLOC_MAX_NODES)
+        return fail(CS_ERR_SIZE, "cs_links_build_noalloc: %lld nodes exceed the static scratch limit of %lld nodes; "
+                    "use cs_links_count / cs_links_fill with a caller-provided scratch buffer", (long long)n,
+                    (long long)NOALLOC_MAX_NODES);
+    if (gmax_cap < 0 || int64_t(Q) * (n + gmax_cap) >= (int64_t(1) << 31))
+        return fail(CS_ERR_SIZE, "cs_links_build_noalloc: gmax_cap %lld (27 * (n + gmax_cap) must stay below 2^31)",
+                    (long long)gmax_cap);
+    if (n_out < 1) return fail(CS_ERR_ARG, "cs_links_build_noalloc: n_out %d", n_out);
+    if (n == 0) return CS_OK;
+    if (!nbr || !q || !links || (gmax_cap > 0 && (!gnode || !ginfo || !gq)))
+        return fail(CS_ERR_ARG, "cs_links_build_noalloc: null buffer");
+    int64_t* scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc != CS_OK) return rc;
+    const Layout l = layout(n);
+    int64_t* part = scratch;
+    int64_t* status = scratch + int64_t(Q) * (NOALLOC_TILES + 1);
+    cudaStream_t st = as_stream(stream);
+    k_ghost_count<<<dim3(unsigned(l.tiles), Q), T_THREADS, 0, st>>>(nbr, n, l.tiles, part);
+    CS_CHECK_LAUNCH("k_ghost_count");
+    k_ghost_scan<<<Q, 1024, 0, st>>>(part, l.tiles);
+    CS_CHECK_LAUNCH("k_ghost_scan");
+    for (int i = 0; i < Q; ++i)
+        CS_CUDA(cudaMemcpyAsync(ghosts + i, part + int64_t(i) * (l.tiles + 1) + l.tiles, sizeof(int64_t),
+                                cudaMemcpyDeviceToHost, st));
+    CS_CUDA(cudaStreamSynchronize(st));
+    int64_t gmax = 0;
+    for (int i = 0; i < Q; ++i) gmax = std::max(gmax, ghosts[i]);
+    if (gmax > gmax_cap)
+        return fail(CS_ERR_SIZE, "cs_links_build_noalloc: %lld ghost slots needed in one direction, gmax_cap is "
+                    "%lld (ghosts holds the counts)", (long long)gmax, (long long)gmax_cap);
+    unsigned long long init[2] = {0ull, ~0ull};
+    CS_CUDA(cudaMemcpyAsync(status, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    k_ghost_fill<<<dim3(unsigned(l.tiles), Q), T_THREADS, 0, st>>>(nbr, q, n, n_out, gmax_cap, l.tiles, part, links,
+                                                                   gnode, ginfo, gq,
+                                                                   reinterpret_cast<unsigned long long*>(status));
+    CS_CHECK_LAUNCH("k_ghost_fill");
+    unsigned long long res[2];
+    CS_CUDA(cudaMemcpyAsync(res, status, sizeof(res), cudaMemcpyDeviceToHost, st));
+    CS_CUDA(cudaStreamSynchronize(st));
+    if (res[0]) {
+        const long long t = (long long)res[1];
+        return fail(CS_ERR_ARG, "cs_links_build_noalloc: %llu invalid entries; first at link %lld node %lld (sources "
+                    "must be < N, outlet codes < n_out = %d, wall q finite and >= 0)", res[0], t / n, t % n, n_out);
+    }
+    return CS_OK;
+}

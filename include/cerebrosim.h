@@ -110,6 +110,24 @@ int cs_links_count(const int32_t* nbr, int64_t n, void* scratch, int64_t* ghosts
 int cs_links_fill(const int32_t* nbr, const float* q, int64_t n, int32_t n_out, int64_t gmax, void* scratch,
                   int32_t* links, int32_t* gnode, int32_t* ginfo, float* gq, int64_t* status, void* stream);
 
+/* The link-table build of cs_links_count + cs_links_fill in one call that allocates nothing. This entry point has
+ * no counterpart in the reference. It is for callers that cannot allocate device memory themselves — a plugin whose
+ * host application owns all device memory and hands it only the input and output buffers, or a process whose
+ * fixed device-memory budget is already committed — and so cannot provide the scratch buffer cs_links_count /
+ * cs_links_fill need.
+ * The scratch (per-tile ghost counts and two status words, about 885 KB) is a static array inside the library:
+ * every GPU that loads the library holds it until the process exits. n is limited to 16,777,216 nodes (2^24);
+ * larger lattices get CS_ERR_SIZE and must use cs_links_count / cs_links_fill. The caller passes the outputs sized
+ * for gmax_cap ghost slots per direction (tables 27 * gmax_cap, gnode pre-filled with -1 so that unused slots are
+ * marked); ghosts (HOST, 27 int64) receives the counts, and CS_ERR_SIZE comes back (with the counts) when a
+ * direction needs more than gmax_cap. The ghost tables then have stride gmax_cap: use it as gmax in the step.
+ * The first call on a device looks up the array's device address (with that device current) and caches it; make
+ * that first call before any stream capture. Every call shares the one array and resets what it reads before
+ * reading it, but calls that overlap on the GPU (other streams, other host threads) race on it. Synchronises
+ * `stream`; makes no cudaMalloc, cudaFree or other allocating call. */
+int cs_links_build_noalloc(const int32_t* nbr, const float* q, int64_t n, int32_t n_out, int64_t gmax_cap,
+                           int32_t* links, int32_t* gnode, int32_t* ginfo, float* gq, int64_t* ghosts, void* stream);
+
 /* Inverse of cs_links_fill for checking: the reference's nbr codes and q (0.5 on non-wall links, lbm.py:281). */
 int cs_links_decode(const int32_t* links, const int32_t* ginfo, const float* gq, int64_t n, int64_t gmax,
                     int32_t* nbr, float* q, void* stream);
