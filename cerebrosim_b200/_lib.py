@@ -9,7 +9,8 @@ import os
 import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libcerebrosim_b200.so")
+# the in-tree build; CEREBROSIM_B200_LIB may name another build of the same ABI (checked at load)
+LIB_PATH = os.environ.get("CEREBROSIM_B200_LIB") or os.path.join(HERE, "libcerebrosim_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "cerebrosim.h")
 
 CS_OK, CS_ERR_ARG, CS_ERR_CUDA, CS_ERR_SIZE, CS_ERR_DEVICE = 0, 1, 2, 3, 4

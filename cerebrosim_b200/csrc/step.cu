@@ -321,18 +321,20 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
         for (int k = 0; k < 6; ++k) g[k] = __ldg(grad_src(d, vin, 1 + k, k / 2, lk[1 + k]));
     }
 
+    // TRT needs f_i and f_opp(i); the body-force path keeps the populations for the per-link evaluation below
+    constexpr bool KEEP = MODEL == CS_MODEL_TRT || FORCE;
     Moments m;
-    float fk[MODEL == CS_MODEL_TRT ? Q : 1];
+    float fk[KEEP ? Q : 1];
     const float v0 = Pop<ST>::ld(fin, uint32_t(lk[0]), wgt(0));
     m.dr = v0;
-    if constexpr (MODEL == CS_MODEL_TRT) fk[0] = v0;
+    if constexpr (KEEP) fk[0] = v0;
     Unroll<0, 13>::run([&](auto pc) {
         constexpr int I = 1 + 2 * decltype(pc)::value;
         constexpr int O = Lat::opp(I);
         const float v = Pop<ST>::ld(fin, uint32_t(I) * NP + uint32_t(lk[I]), wgt(I));
         const float vo = Pop<ST>::ld(fin, uint32_t(O) * NP + uint32_t(lk[O]), wgt(O));
         m.add_pair<I>(v, vo);
-        if constexpr (MODEL == CS_MODEL_TRT) {
+        if constexpr (KEEP) {
             fk[I] = v;
             fk[O] = vo;
         }
@@ -380,9 +382,28 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
 
     const Cubic cu3(ux, uy, uz);
     if constexpr (MODEL == CS_MODEL_REGULARISED) {
-        const float d3 = dr * (1.0f / 3.0f);
-        float pxx = m.pxx - d3 - ux * ux, pyy = m.pyy - d3 - uy * uy, pzz = m.pzz - d3 - uz * uz;
-        float pxy = m.pxy - ux * uy, pxz = m.pxz - ux * uz, pyz = m.pyz - uy * uz;
+        float pxx, pyy, pzz, pxy, pxz, pyz;
+        if constexpr (FORCE) {
+            // with a body force, P link by link as the reference sums it (lbm.py:220-223): a slowly forced steady
+            // state (Poiseuille at tau ~ 0.505, forces ~1e-7) keeps the FP32 rounding of this order
+            pxx = pyy = pzz = pxy = pxz = pyz = 0.0f;
+            Unroll<0, Q>::run([&](auto ic) {
+                constexpr int I = decltype(ic)::value;
+                constexpr int x = Lat::cx(I), y = Lat::cy(I), z = Lat::cz(I);
+                const float cu = cdot<I>(ux, uy, uz);
+                const float sv = fk[I] - wgt(I) * (dr + 3.0f * cu + 4.5f * cu * cu - 1.5f * usq);
+                if (x) pxx += sv;
+                if (y) pyy += sv;
+                if (z) pzz += sv;
+                if (x && y) pxy += float(x * y) * sv;
+                if (x && z) pxz += float(x * z) * sv;
+                if (y && z) pyz += float(y * z) * sv;
+            });
+        } else {
+            const float d3 = dr * (1.0f / 3.0f);
+            pxx = m.pxx - d3 - ux * ux, pyy = m.pyy - d3 - uy * uy, pzz = m.pzz - d3 - uz * uz;
+            pxy = m.pxy - ux * uy, pxz = m.pxz - ux * uz, pyz = m.pyz - uy * uz;
+        }
         if (d.sigma < 1.0f) {
             // hybrid regularisation (lbm.py:224-229): G[a][b] = du_b/dx_a from the previous step's velocity
             float gr[3][3];
@@ -408,7 +429,38 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
         pzz -= edz;
         const float trp = (pxx + pyy + pzz) * (1.0f / 3.0f);
         const float k_ne = 1.0f - om, k_src = 1.0f - 0.5f * om;
-        // f_out = feq + (1 - om) fneq + (1 - om/2) src (lbm.py:236-240) regrouped as w (A + E +- O)
+        if constexpr (FORCE) {
+            // f_out = feq + (1 - om) fneq + (1 - om/2) src per link in the reference's order (lbm.py:232-240)
+            const float w0 = wgt(0);
+            Pop<ST>::st(fout, uint32_t(n), w0, w0 * (dr - 1.5f * usq) + k_ne * (w0 * (4.5f * (0.0f - trp))) +
+                                                   k_src * (w0 * (-3.0f * uF)));
+            Unroll<0, 13>::run([&](auto pc) {
+                constexpr int I = 1 + 2 * decltype(pc)::value;
+                constexpr int O = Lat::opp(I);
+                const float cu = cdot<I>(ux, uy, uz), cF = cdot<I>(Fx, Fy, Fz);
+                const float cpc = quad<I>(pxx, pyy, pzz, 2.0f * pxy, 2.0f * pxz, 2.0f * pyz);
+                const float h = t3 * cu3.template h3<I>();
+                const float w = wgt(I);
+                const float feq_i = w * (dr + 3.0f * cu + 4.5f * cu * cu - 1.5f * usq + h);
+                const float feq_o = w * (dr - 3.0f * cu + 4.5f * cu * cu - 1.5f * usq - h);
+                const float fneq_i = w * (4.5f * (cpc - trp) - 1.5f * cF);
+                const float fneq_o = w * (4.5f * (cpc - trp) + 1.5f * cF);
+                const float src_i = w * (3.0f * cF + 9.0f * cu * cF - 3.0f * uF);
+                const float src_o = w * (-3.0f * cF + 9.0f * cu * cF - 3.0f * uF);
+                Pop<ST>::st(fout, uint32_t(I) * NP + uint32_t(n), w, feq_i + k_ne * fneq_i + k_src * src_i);
+                Pop<ST>::st(fout, uint32_t(O) * NP + uint32_t(n), w, feq_o + k_ne * fneq_o + k_src * src_o);
+            });
+            vout[n] = ux;
+            vout[N + n] = uy;
+            vout[2 * N + n] = uz;
+            d.rho[n] = dr;
+            ux_o = ux;
+            uy_o = uy;
+            uz_o = uz;
+            return;
+        }
+        // without a force: f_out = feq + (1 - om) fneq + (1 - om/2) src (lbm.py:236-240) regrouped as
+        // w (A + E +- O), each pair's terms evaluated once
         const float A = dr - 1.5f * usq - 4.5f * k_ne * trp - 3.0f * k_src * uF;
         const float s = 4.5f * k_ne;
         const float qxx = s * pxx, qyy = s * pyy, qzz = s * pzz;
