@@ -44,8 +44,17 @@ class StepDesc(ctypes.Structure):
                 ("period", ctypes.c_int32), ("ramp", ctypes.c_int32),
                 ("n_open", ctypes.c_int32), ("n_flux", ctypes.c_int64), ("flux_idx", ctypes.c_void_p),
                 ("flux_w", ctypes.c_void_p), ("flux_slot", ctypes.c_void_p), ("flux_block", ctypes.c_void_p),
-                ("q_acc", ctypes.c_void_p), ("q_last", ctypes.c_void_p), ("p_out64", ctypes.c_void_p),
+                ("q_part", ctypes.c_void_p), ("fb_list", ctypes.c_void_p), ("n_fb", ctypes.c_int32),
+                ("q_last", ctypes.c_void_p), ("p_out64", ctypes.c_void_p),
                 ("r_out", ctypes.c_void_p), ("pref", ctypes.c_double), ("alpha", ctypes.c_double)]
+
+
+class BatchDesc(ctypes.Structure):
+    _fields_ = [("n_inst", ctypes.c_int32), ("storage", ctypes.c_int32), ("model", ctypes.c_int32),
+                ("gal", ctypes.c_int32), ("force", ctypes.c_int32), ("any_open", ctypes.c_int32),
+                ("block", ctypes.c_int32), ("grid_bulk", ctypes.c_int32), ("grid_bnd", ctypes.c_int32),
+                ("bulk_items", ctypes.c_int32), ("bnd_items", ctypes.c_int32), ("descs", ctypes.c_void_p),
+                ("parity", ctypes.c_void_p), ("bulk_prefix", ctypes.c_void_p), ("bnd_prefix", ctypes.c_void_p)]
 
 
 _P = ctypes.c_void_p
@@ -68,6 +77,9 @@ SIGNATURES = {
     "cs_compress_expand": (_I32, [_P, _P, _P, _I64, _I64, _P, _P]),
     "cs_flux_blocks": (_I32, [_P, _I64, _I64, _I32, _P, _P]),
     "cs_step": (_I32, [ctypes.POINTER(StepDesc), _I32, _I32, _P]),
+    "cs_step_check": (_I32, [ctypes.POINTER(StepDesc)]),
+    "cs_batch_step": (_I32, [ctypes.POINTER(BatchDesc), _I32, _I32, _P]),
+    "cs_batch_graph_capture": (_I32, [ctypes.POINTER(BatchDesc), _I32, _I32, _P, ctypes.POINTER(_P)]),
     "cs_graph_capture": (_I32, [ctypes.POINTER(StepDesc), _I32, _I32, _P, ctypes.POINTER(_P)]),
     "cs_graph_launch": (_I32, [_P, _P]),
     "cs_graph_destroy": (_I32, [_P]),
@@ -99,7 +111,8 @@ def load():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if lib.cs_abi_sizeof(0) != ctypes.sizeof(Opening) or lib.cs_abi_sizeof(1) != ctypes.sizeof(StepDesc):
+    if (lib.cs_abi_sizeof(0) != ctypes.sizeof(Opening) or lib.cs_abi_sizeof(1) != ctypes.sizeof(StepDesc)
+            or lib.cs_abi_sizeof(3) != ctypes.sizeof(BatchDesc)):
         raise ImportError("libcerebrosim_b200.so ABI mismatch: rebuild the library")
     _lib = lib
     return lib

@@ -1,0 +1,170 @@
+"""Many vessels in one launch: `BatchSolver` advances several `lbm.Solver` / `ArterySolver` instances together.
+
+The reference runs one simulation per GPU process and scales out with a Slurm job array of one-GPU jobs
+(slurm/submit_all.sh:21,36-38, slurm/config.sh:20); small vessels then leave most of a B200 idle. Here the
+instances' node lists are concatenated into one work list and a persistent kernel per step covers all of them
+(csrc/step.cu, `cs_batch_step`): each block takes work items — a bulk block or a boundary block of some instance —
+and reads that instance's descriptor (buffers, clock, drive, outlet pressures, coupling) into shared memory. The
+arithmetic of every instance is the single-lattice kernels' own, so an instance evolves exactly as it would alone.
+
+Instances may join and leave between runs (continuous batching): each keeps its own buffer parity, and the batch
+descriptor table is rebuilt when the membership or an instance's parameters change.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check
+from .lbm import ctypes_void
+
+BOUNDARY_THREADS = 256
+
+
+class BatchSolver:
+    """Advance `solvers` (same device, storage format, collision model and Galilean setting) together.
+
+    block: threads per bulk block for every member (their flux partitions are rebuilt to match).
+    persistent: size the grids to the GPU (SMs x resident blocks) and loop over work items, instead of one block
+    per work item."""
+
+    def __init__(self, solvers=(), block=256, persistent=True, device=None):
+        self.members = []
+        self.block = int(block)
+        self.persistent = bool(persistent)
+        self.dev = None
+        self.cur = 0
+        self.steps = 0
+        self.graphs = {}
+        self._parity = []
+        self._key = None
+        self.stream = None
+        for s in solvers:
+            self.add(s)
+
+    # --- membership
+    def add(self, s):
+        """Join an instance; it continues from its own state and step count."""
+        if self.dev is None:
+            self.dev = s.dev
+            self.stream = torch.cuda.Stream(self.dev)
+        if s.dev != self.dev:
+            raise ValueError("all instances of a batch must be on one device")
+        if self.members:
+            m0 = self.members[0]
+            if (s.storage, s.model, s.gal) != (m0.storage, m0.model, m0.gal):
+                raise ValueError("instances of a batch share the storage format, collision model and Galilean setting")
+        if s.block != self.block:
+            s.block = self.block
+            if hasattr(s, "_set_flux_blocks"):
+                s._set_flux_blocks()
+            s._drop_graphs()
+        self.members.append(s)
+        self._parity.append(s.cur ^ self.cur)
+        self._key = None
+
+    def remove(self, s):
+        """Leave the batch; the instance keeps its state and can run alone or join another batch."""
+        k = self.members.index(s)
+        self.stream.synchronize()
+        del self.members[k]
+        del self._parity[k]
+        self._key = None
+
+    # --- descriptor table
+    def _drop_graphs(self):
+        lib = _lib.load()
+        for g in self.graphs.values():
+            lib.cs_graph_destroy(g)
+        self.graphs = {}
+
+    def _refresh(self):
+        """(Re)build the device descriptor table when members or their parameters changed."""
+        lib = _lib.load()
+        descs = [m._desc() for m in self.members]
+        for d in descs:
+            check(lib.cs_step_check(ctypes.byref(d)))
+        raw = b"".join(bytes(d) for d in descs)
+        key = (raw, tuple(self._parity))
+        if key == self._key:
+            return
+        self._drop_graphs()
+        n = len(self.members)
+        bulk = [-(-m.N // self.block) if m.N else 0 for m in self.members]
+        bnd = [27 * max(1, -(-m.gmax // BOUNDARY_THREADS)) for m in self.members]
+        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+            self._descs = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(self.dev)
+            self._par = torch.tensor(self._parity, dtype=torch.int32, device=self.dev)
+            self._bulk_prefix = torch.tensor(np.concatenate([[0], np.cumsum(bulk)]), dtype=torch.int32,
+                                             device=self.dev)
+            self._bnd_prefix = torch.tensor(np.concatenate([[0], np.cumsum(bnd)]), dtype=torch.int32,
+                                            device=self.dev)
+        m0 = self.members[0]
+        b = _lib.BatchDesc()
+        b.n_inst = n
+        b.storage, b.model, b.gal = _lib.STORE[m0.storage], m0.model, m0.gal
+        b.force = int(any(any(x != 0.0 for x in m.force) for m in self.members))
+        b.any_open = int(any(getattr(m, "n_open", 0) > 0 for m in self.members))
+        b.block = self.block
+        b.bulk_items, b.bnd_items = int(sum(bulk)), int(sum(bnd))
+        sms = torch.cuda.get_device_properties(self.dev).multi_processor_count
+        b.grid_bulk = sms * 3 if self.persistent else 0          # 3 resident bulk blocks per SM
+        b.grid_bnd = sms * 8 if self.persistent else 0           # 8 resident boundary blocks per SM
+        b.descs, b.parity = self._descs.data_ptr(), self._par.data_ptr()
+        b.bulk_prefix, b.bnd_prefix = self._bulk_prefix.data_ptr(), self._bnd_prefix.data_ptr()
+        self.desc = b
+        self._key = key
+
+    # --- stepping
+    def _sync_in(self):
+        self.stream.wait_stream(torch.cuda.current_stream(self.dev))
+        for m in self.members:
+            self.stream.wait_stream(m.stream)
+
+    def _sync_out(self):
+        torch.cuda.current_stream(self.dev).wait_stream(self.stream)
+        for m in self.members:
+            m.stream.wait_stream(self.stream)
+
+    def run(self, steps, chunk=200):
+        """Advance every member `steps` steps (CUDA graphs of `chunk` batched steps; chunk even)."""
+        if not self.members:
+            return
+        self._refresh()
+        lib = _lib.load()
+        chunk += chunk % 2
+        full, rest = divmod(int(steps), chunk)
+        self._sync_in()
+        sp = ctypes_void(self.stream.cuda_stream)
+        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+            if full:
+                key = (self.cur, chunk)
+                if key not in self.graphs:
+                    g = ctypes.c_void_p()
+                    check(lib.cs_batch_graph_capture(ctypes.byref(self.desc), self.cur, chunk, sp, ctypes.byref(g)))
+                    self.graphs[key] = g
+                for _ in range(full):
+                    check(lib.cs_graph_launch(self.graphs[key], sp))
+            if rest:
+                check(lib.cs_batch_step(ctypes.byref(self.desc), self.cur, rest, sp))
+                if rest % 2:
+                    self.cur = 1 - self.cur
+        self._sync_out()
+        self.steps += int(steps)
+        for m, p in zip(self.members, self._parity):
+            m.cur = self.cur ^ p
+            m.steps += int(steps)
+
+    def synchronize(self):
+        self.stream.synchronize()
+
+    @property
+    def nodes(self):
+        return sum(m.N for m in self.members)
+
+    def __del__(self):
+        try:
+            self._drop_graphs()
+        except Exception:
+            pass

@@ -43,6 +43,7 @@ extern "C" size_t cs_abi_sizeof(int32_t which) {
         case 0: return sizeof(cs_opening);
         case 1: return sizeof(cs_step_desc);
         case 2: return CS_SEG_STRIDE;
+        case 3: return sizeof(cs_batch_desc);
         default: return 0;
     }
 }

@@ -205,12 +205,14 @@ __device__ __forceinline__ float cdot(float ax, float ay, float az) {
 }
 
 // ---- 1. boundary-link kernel and clock ----------------------------------------------------------------------------
+// Block (bx, by) of a lattice's boundary-link grid: by = direction, bx = chunk of its ghost slots. Called by every
+// thread of the block (it synchronises the block once).
 template <int ST>
-__global__ void __launch_bounds__(B_THREADS) k_boundary(const cs_step_desc d, const int a) {
+__device__ __forceinline__ void boundary_body(const cs_step_desc& d, const int a, const int bx, const int by) {
     __shared__ float s_drive;
     // the ghost table is static: read it before waiting for the previous kernel of the stream
-    const int i = blockIdx.y;
-    const int64_t g = int64_t(blockIdx.x) * B_THREADS + threadIdx.x;
+    const int i = by;
+    const int64_t g = int64_t(bx) * B_THREADS + threadIdx.x;
     const int64_t slot = int64_t(i) * d.gmax + g;
     const bool live = g < d.gmax;
     const int32_t node = live ? __ldg(d.gnode + slot) : -1;
@@ -220,7 +222,7 @@ __global__ void __launch_bounds__(B_THREADS) k_boundary(const cs_step_desc d, co
     if (threadIdx.x == 0) {
         const int t = d.tick[a];
         s_drive = drive_value(d, t);
-        if (blockIdx.x == 0 && blockIdx.y == 0) {
+        if (bx == 0 && by == 0) {
             *d.drive = s_drive;
             d.tick[1 - a] = t + 1;
         }
@@ -262,6 +264,11 @@ __global__ void __launch_bounds__(B_THREADS) k_boundary(const cs_step_desc d, co
         v = -fo + 2.0f * w * (3.0f * __ldg(d.p_out + (CS_OUTLET0 - info)) + 4.5f * cu * cu - 1.5f * usq);
     }
     Pop<ST>::st(d.f[a], uint32_t(i) * NP + uint32_t(d.n + g), w, v);
+}
+
+template <int ST>
+__global__ void __launch_bounds__(B_THREADS) k_boundary(const cs_step_desc d, const int a) {
+    boundary_body<ST>(d, a, blockIdx.x, blockIdx.y);
 }
 
 // ---- 2. bulk kernel -----------------------------------------------------------------------------------------------
@@ -506,11 +513,12 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
     uz_o = uz;
 }
 
+// Block bx of a lattice's bulk grid (nodes bx * blockDim .. + blockDim - 1). Called by every thread of the block.
 template <int ST, int MODEL, bool GAL, bool FORCE>
-__global__ void __launch_bounds__(MAX_BLOCK, MIN_BLOCKS) k_bulk(const cs_step_desc d, const int a) {
+__device__ __forceinline__ void bulk_body(const cs_step_desc& d, const int a, const int bx) {
     __shared__ float s_u[3][MAX_BLOCK];
     __shared__ double s_q[MAX_OPEN];
-    const int32_t n0 = int32_t(blockIdx.x) * int32_t(blockDim.x);
+    const int32_t n0 = int32_t(bx) * int32_t(blockDim.x);
     const int32_t n = n0 + int32_t(threadIdx.x);
     float ux = 0.f, uy = 0.f, uz = 0.f;
     if (n < d.n) node_update<ST, MODEL, GAL, FORCE>(d, a, n, ux, uy, uz);
@@ -518,34 +526,74 @@ __global__ void __launch_bounds__(MAX_BLOCK, MIN_BLOCKS) k_bulk(const cs_step_de
     launch_dependents();
 
     if (d.n_open > 0) {
-        // slab flux Q_k += u . w over this block's flux entries (simulate.py:65-69), FP64
-        const int e0 = __ldg(d.flux_block + blockIdx.x), e1 = __ldg(d.flux_block + blockIdx.x + 1);
+        // slab flux Q_k = sum u . w over this block's flux entries (simulate.py:65-69), FP64, in a fixed order: each
+        // thread sums its entries, warps reduce by shuffles, warp 0 adds the warps in order; the block's partial
+        // sums go to its own row of q_part, which k_bc adds up in a fixed order too (no atomics: bit-reproducible)
+        const int e0 = __ldg(d.flux_block + bx), e1 = __ldg(d.flux_block + bx + 1);
         if (e1 > e0) {
             s_u[0][threadIdx.x] = ux;
             s_u[1][threadIdx.x] = uy;
             s_u[2][threadIdx.x] = uz;
-            if (threadIdx.x < MAX_OPEN) s_q[threadIdx.x] = 0.0;
             __syncthreads();
+            double acc[MAX_OPEN];
+#pragma unroll
+            for (int k = 0; k < MAX_OPEN; ++k) acc[k] = 0.0;
             for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
                 const int loc = __ldg(d.flux_idx + e) - n0;
                 if (loc < 0 || loc >= int(blockDim.x)) continue;  // partition built for another block size
                 const float* w = d.flux_w + 3 * int64_t(e);
                 const double v = double(s_u[0][loc]) * double(__ldg(w)) + double(s_u[1][loc]) * double(__ldg(w + 1)) +
                                  double(s_u[2][loc]) * double(__ldg(w + 2));
-                atomicAdd(&s_q[__ldg(d.flux_slot + e)], v);
+                const int slot = __ldg(d.flux_slot + e);
+#pragma unroll
+                for (int k = 0; k < MAX_OPEN; ++k) acc[k] += slot == k ? v : 0.0;
+            }
+            __shared__ double s_w[MAX_BLOCK / 32][MAX_OPEN];
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+            for (int k = 0; k < MAX_OPEN; ++k) {
+                double x = acc[k];
+                for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+                if (lane == 0) s_w[warp][k] = x;
             }
             __syncthreads();
-            if (threadIdx.x < d.n_open && s_q[threadIdx.x] != 0.0) atomicAdd(d.q_acc + threadIdx.x, s_q[threadIdx.x]);
+            if (threadIdx.x < d.n_open) {
+                double t = 0.0;
+                for (int w = 0; w < int(blockDim.x) / 32; ++w) t += s_w[w][threadIdx.x];
+                d.q_part[int64_t(bx) * MAX_OPEN + threadIdx.x] = t;
+            }
         }
     }
 }
 
+template <int ST, int MODEL, bool GAL, bool FORCE>
+__global__ void __launch_bounds__(MAX_BLOCK, MIN_BLOCKS) k_bulk(const cs_step_desc d, const int a) {
+    bulk_body<ST, MODEL, GAL, FORCE>(d, a, blockIdx.x);
+}
+
 // ---- 3. outlet resistances ----------------------------------------------------------------------------------------
-__global__ void k_bc(const cs_step_desc d) {
-    // simulate.py:76-82 in FP64; the drive of this step was stored by the boundary kernel
+constexpr int BC_THREADS = 256;
+
+// simulate.py:76-82 in FP64 (one block of BC_THREADS threads); the drive of this step was stored by the boundary
+// kernel. Q_k = the flux blocks' partial sums, added by a fixed-shape tree (the same order at every step and run).
+__device__ __forceinline__ void bc_body(const cs_step_desc& d) {
+    __shared__ double s_red[BC_THREADS];
+    __shared__ double s_q[MAX_OPEN];
+    for (int k = 0; k < d.n_open; ++k) {
+        double t = 0.0;
+        for (int j = threadIdx.x; j < d.n_fb; j += BC_THREADS) t += d.q_part[int64_t(__ldg(d.fb_list + j)) * MAX_OPEN + k];
+        s_red[threadIdx.x] = t;
+        __syncthreads();
+        for (int h = BC_THREADS / 2; h > 0; h >>= 1) {
+            if (threadIdx.x < h) s_red[threadIdx.x] += s_red[threadIdx.x + h];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) s_q[k] = s_red[0];
+        __syncthreads();
+    }
     const int k = threadIdx.x;
     if (k >= d.n_open) return;
-    const double qk = d.q_acc[k];
+    const double qk = s_q[k];
     d.q_last[k] = qk;
     if (k == 0) {
         const float dv = *d.drive;
@@ -556,8 +604,9 @@ __global__ void k_bc(const cs_step_desc d) {
         d.p_out64[k] = p;
         d.p_out[k] = float(p);
     }
-    d.q_acc[k] = 0.0;
 }
+
+__global__ void k_bc(const cs_step_desc d) { bc_body(d); }
 
 using StepFn = void (*)(const cs_step_desc, const int);
 
@@ -610,7 +659,8 @@ int validate(const cs_step_desc* d) {
     if (d->gmax > 0 && (!d->gnode || !d->ginfo || !d->gq)) return fail(CS_ERR_ARG, "cs_step: null ghost table");
     if (d->n_open < 0 || d->n_open > MAX_OPEN || d->n_open > d->n_out)
         return fail(CS_ERR_ARG, "cs_step: n_open %d (at most %d and at most n_out %d)", d->n_open, MAX_OPEN, d->n_out);
-    if (d->n_open > 0 && (!d->flux_block || !d->q_acc || !d->q_last || !d->p_out64 || !d->r_out ||
+    if (d->n_open > 0 && (!d->flux_block || !d->q_part || !d->q_last || !d->p_out64 || !d->r_out ||
+                          d->n_fb < 0 || (d->n_fb > 0 && !d->fb_list) ||
                           (d->n_flux > 0 && (!d->flux_idx || !d->flux_w || !d->flux_slot))))
         return fail(CS_ERR_ARG, "cs_step: null flux buffer");
     return CS_OK;
@@ -648,7 +698,7 @@ int launch_steps(const cs_step_desc* d, int a, int steps, cudaStream_t st) {
             if (rc != CS_OK) return rc;
         }
         if (d->n_open > 0) {
-            k_bc<<<1, 32, 0, st>>>(*d);
+            k_bc<<<1, BC_THREADS, 0, st>>>(*d);
             CS_CHECK_LAUNCH("k_bc");
         }
         a = 1 - a;
@@ -732,5 +782,171 @@ extern "C" int cs_graph_destroy(void* graph) {
     cudaError_t e = cudaGraphExecDestroy(g->exec);
     delete g;
     if (e != cudaSuccess) return fail(CS_ERR_CUDA, "cudaGraphExecDestroy: %s", cudaGetErrorString(e));
+    return CS_OK;
+}
+
+extern "C" int cs_step_check(const cs_step_desc* d) { return validate(d); }
+
+// ---- batched step -------------------------------------------------------------------------------------------------
+namespace cs {
+namespace {
+
+// Largest i in [0, n) with prefix[i] <= item.
+__device__ __forceinline__ int find_instance(const int32_t* prefix, int n, int item) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= item) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// The block's work item -> instance and local index, and the instance's descriptor copied to shared memory.
+__device__ __forceinline__ void take_item(const cs_batch_desc& b, const int32_t* prefix, int item, cs_step_desc& sd,
+                                          int& inst, int& local) {
+    __shared__ int s_inst, s_local;
+    if (threadIdx.x == 0) {
+        const int i = find_instance(prefix, b.n_inst, item);
+        s_inst = i;
+        s_local = item - __ldg(prefix + i);
+    }
+    __syncthreads();
+    inst = s_inst;
+    local = s_local;
+    const int* src = reinterpret_cast<const int*>(b.descs + inst);
+    int* dst = reinterpret_cast<int*>(&sd);
+    for (int k = threadIdx.x; k < int(sizeof(cs_step_desc) / sizeof(int)); k += blockDim.x) dst[k] = __ldg(src + k);
+    __syncthreads();
+}
+
+template <int ST>
+__global__ void __launch_bounds__(B_THREADS) k_boundary_batch(const cs_batch_desc b, const int a) {
+    __shared__ cs_step_desc sd;
+    for (int item = blockIdx.x; item < b.bnd_items; item += gridDim.x) {
+        int inst, local;
+        take_item(b, b.bnd_prefix, item, sd, inst, local);
+        const int nbx = int(max(int64_t(1), ceil_div(sd.gmax, B_THREADS)));
+        boundary_body<ST>(sd, a ^ __ldg(b.parity + inst), local % nbx, local / nbx);
+        __syncthreads();
+    }
+}
+
+template <int ST, int MODEL, bool GAL, bool FORCE>
+__global__ void __launch_bounds__(MAX_BLOCK, MIN_BLOCKS) k_bulk_batch(const cs_batch_desc b, const int a) {
+    __shared__ cs_step_desc sd;
+    for (int item = blockIdx.x; item < b.bulk_items; item += gridDim.x) {
+        int inst, local;
+        take_item(b, b.bulk_prefix, item, sd, inst, local);
+        bulk_body<ST, MODEL, GAL, FORCE>(sd, a ^ __ldg(b.parity + inst), local);
+        __syncthreads();
+    }
+}
+
+__global__ void k_bc_batch(const cs_batch_desc b) {
+    __shared__ cs_step_desc sd;
+    const int* src = reinterpret_cast<const int*>(b.descs + blockIdx.x);
+    int* dst = reinterpret_cast<int*>(&sd);
+    for (int k = threadIdx.x; k < int(sizeof(cs_step_desc) / sizeof(int)); k += blockDim.x) dst[k] = __ldg(src + k);
+    __syncthreads();
+    if (sd.n_open > 0) bc_body(sd);
+}
+
+using BatchFn = void (*)(const cs_batch_desc, const int);
+
+template <int ST>
+BatchFn pick_batch_model(int model, int gal, bool force) {
+    if (model == CS_MODEL_REGULARISED) {
+        if (gal) return force ? k_bulk_batch<ST, CS_MODEL_REGULARISED, true, true> : k_bulk_batch<ST, CS_MODEL_REGULARISED, true, false>;
+        return force ? k_bulk_batch<ST, CS_MODEL_REGULARISED, false, true> : k_bulk_batch<ST, CS_MODEL_REGULARISED, false, false>;
+    }
+    if (gal) return force ? k_bulk_batch<ST, CS_MODEL_TRT, true, true> : k_bulk_batch<ST, CS_MODEL_TRT, true, false>;
+    return force ? k_bulk_batch<ST, CS_MODEL_TRT, false, true> : k_bulk_batch<ST, CS_MODEL_TRT, false, false>;
+}
+
+int validate_batch(const cs_batch_desc* b) {
+    if (!b) return fail(CS_ERR_ARG, "cs_batch_step: null descriptor");
+    if (b->n_inst < 1 || !b->descs || !b->parity || !b->bulk_prefix || !b->bnd_prefix)
+        return fail(CS_ERR_ARG, "cs_batch_step: %d instances or null tables", b->n_inst);
+    if (b->storage < 0 || b->storage > 2 || (b->model != CS_MODEL_TRT && b->model != CS_MODEL_REGULARISED))
+        return fail(CS_ERR_ARG, "cs_batch_step: storage %d model %d", b->storage, b->model);
+    if (b->block < 32 || b->block > MAX_BLOCK || b->block % 32)
+        return fail(CS_ERR_ARG, "cs_batch_step: block %d (32..%d, multiple of 32)", b->block, MAX_BLOCK);
+    if (b->bulk_items < 0 || b->bnd_items < b->n_inst * Q || b->grid_bulk < 0 || b->grid_bnd < 0)
+        return fail(CS_ERR_ARG, "cs_batch_step: work items %d / %d", b->bulk_items, b->bnd_items);
+    return CS_OK;
+}
+
+int launch_batch_pdl(BatchFn fn, unsigned grid, unsigned block, cudaStream_t st, const cs_batch_desc& b, int a) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, fn, b, a);
+    if (e != cudaSuccess) return fail(CS_ERR_CUDA, "launch of a batched step kernel failed: %s", cudaGetErrorString(e));
+    return CS_OK;
+}
+
+int launch_batch(const cs_batch_desc* b, int a, int steps, cudaStream_t st) {
+    const bool force = b->force != 0;
+    BatchFn bulk = b->storage == CS_STORE_F16    ? pick_batch_model<CS_STORE_F16>(b->model, b->gal, force)
+                   : b->storage == CS_STORE_BF16 ? pick_batch_model<CS_STORE_BF16>(b->model, b->gal, force)
+                                                 : pick_batch_model<CS_STORE_F32>(b->model, b->gal, force);
+    BatchFn bound = b->storage == CS_STORE_F16    ? k_boundary_batch<CS_STORE_F16>
+                    : b->storage == CS_STORE_BF16 ? k_boundary_batch<CS_STORE_BF16>
+                                                  : k_boundary_batch<CS_STORE_F32>;
+    const unsigned gb = unsigned(b->grid_bnd > 0 ? std::min(b->grid_bnd, b->bnd_items) : b->bnd_items);
+    const unsigned gk = unsigned(b->grid_bulk > 0 ? std::min(b->grid_bulk, b->bulk_items) : b->bulk_items);
+    for (int s = 0; s < steps; ++s) {
+        int rc = launch_batch_pdl(bound, gb, B_THREADS, st, *b, a);
+        if (rc != CS_OK) return rc;
+        if (gk > 0) {
+            rc = launch_batch_pdl(bulk, gk, unsigned(b->block), st, *b, a);
+            if (rc != CS_OK) return rc;
+        }
+        if (b->any_open) {
+            k_bc_batch<<<unsigned(b->n_inst), BC_THREADS, 0, st>>>(*b);
+            CS_CHECK_LAUNCH("k_bc_batch");
+        }
+        a = 1 - a;
+    }
+    return CS_OK;
+}
+
+}  // namespace
+}  // namespace cs
+
+extern "C" int cs_batch_step(const cs_batch_desc* b, int32_t a, int32_t steps, void* stream) {
+    int rc = validate_batch(b);
+    if (rc != CS_OK) return rc;
+    if ((a != 0 && a != 1) || steps < 0) return fail(CS_ERR_ARG, "cs_batch_step: a %d steps %d", a, steps);
+    return launch_batch(b, a, steps, as_stream(stream));
+}
+
+extern "C" int cs_batch_graph_capture(const cs_batch_desc* b, int32_t a, int32_t steps, void* stream, void** graph) {
+    int rc = validate_batch(b);
+    if (rc != CS_OK) return rc;
+    if ((a != 0 && a != 1) || steps < 1 || !graph)
+        return fail(CS_ERR_ARG, "cs_batch_graph_capture: a %d steps %d", a, steps);
+    cudaStream_t st = as_stream(stream);
+    if (st == nullptr) return fail(CS_ERR_ARG, "cs_batch_graph_capture: the legacy default stream cannot be captured");
+    CS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    rc = launch_batch(b, a, steps, st);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc != CS_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(CS_ERR_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(e));
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(CS_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    *graph = new Graph{ex};
     return CS_OK;
 }

@@ -2,9 +2,10 @@
 
 `ArterySolver(lat, nu_lu, flux, R_lu, pref_lu, alpha, **kw)` keeps the reference constructor. Per step, after the
 collision, the slab flux Q_k = sum u . w over each open end's flux cells is reduced and the outlet pressures are
-relaxed towards R_k Q_k - pref (simulate.py:65-82). Here that work is fused into the step kernel itself (one
-launch per step instead of four) and runs in FP64: q_acc / Qlast / p_out64 are double, p_out (read by the outlet
-links) is the float32 image of p_out64.
+relaxed towards R_k Q_k - pref (simulate.py:65-82). Here the flux is reduced inside the bulk kernel by the blocks
+that hold slab cells and k_bc adds the blocks' partial sums, both in FP64 and in a fixed order, so a run is
+bit-reproducible; Qlast / p_out64 are double, p_out (read by the outlet links) is the float32 image of p_out64, and
+Qacc (the reference's accumulator, zero between steps) is kept as a zero array.
 
 Device state is exposed through `DeviceArray`, which keeps the reference's `.numpy()` / `.zero_()` / `.assign()`
 access pattern on top of a torch tensor.
@@ -85,13 +86,20 @@ class ArterySolver(Solver):
         self._set_flux_blocks()
 
     def _set_flux_blocks(self):
+        """Partition the sorted flux list by bulk block (for the current block size): each block that holds flux
+        entries writes its partial sums to its own row of q_part; fb_list names those blocks in ascending order."""
         nb = max(1, -(-self.N // self.block))
+        idx = self.f_idx.cpu().numpy()
+        fb = np.unique(idx // self.block).astype(np.int32) if len(idx) else np.zeros(0, np.int32)
         with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
             self._flux_block = torch.empty(nb + 1, dtype=torch.int32, device=self.dev)
             check(_lib.load().cs_flux_blocks(ctypes.c_void_p(self.f_idx.data_ptr() if len(self.f_idx) else 0),
                                              len(self.f_idx), self.N, self.block,
                                              ctypes.c_void_p(self._flux_block.data_ptr()),
                                              ctypes_void(self.stream.cuda_stream)))
+            self._fb_list = torch.as_tensor(fb if len(fb) else np.zeros(1, np.int32)).to(self.dev)
+            self._n_fb = len(fb)
+            self._q_part = torch.zeros(nb * self.MAX_OPEN, dtype=torch.float64, device=self.dev)
 
     def _fill_desc(self, d):
         d.n_open = self.n_open
@@ -100,5 +108,6 @@ class ArterySolver(Solver):
         d.flux_w = self.f_w.data_ptr() if len(self.f_idx) else None
         d.flux_slot = self.f_slot.data_ptr() if len(self.f_idx) else None
         d.flux_block = self._flux_block.data_ptr()
-        d.q_acc, d.q_last, d.r_out = self._qacc.data_ptr(), self._qlast.data_ptr(), self._r.data_ptr()
+        d.q_part, d.fb_list, d.n_fb = self._q_part.data_ptr(), self._fb_list.data_ptr(), self._n_fb
+        d.q_last, d.r_out = self._qlast.data_ptr(), self._r.data_ptr()
         d.pref, d.alpha = self.pref, self.alpha

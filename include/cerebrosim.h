@@ -183,7 +183,9 @@ typedef struct cs_step_desc {
     const float* flux_w;     /* weight vector of each entry (n_flux * 3) */
     const int32_t* flux_slot;/* open end of each entry */
     const int32_t* flux_block; /* first flux entry of each bulk block (n_blocks + 1) from cs_flux_blocks */
-    double* q_acc;           /* flux accumulators (n_open), zero between steps */
+    double* q_part;          /* per bulk block partial fluxes (n_blocks * 8), written by the blocks in fb_list */
+    const int32_t* fb_list;  /* the bulk blocks that hold flux entries, ascending (n_fb) */
+    int32_t n_fb;
     double* q_last;          /* flux of the last step (n_open) */
     double* p_out64;         /* FP64 state of the outlet pressures (n_open) */
     const float* r_out;      /* resistance per open end (n_open) */
@@ -198,9 +200,37 @@ int cs_flux_blocks(const int32_t* flux_idx, int64_t n_flux, int64_t n, int32_t b
  * is the boundary-link kernel (when gmax > 0), the bulk kernel and, when n_open > 0, the one-block k_bc kernel. */
 int cs_step(const cs_step_desc* d, int32_t a, int32_t steps, void* stream);
 
+/* Check a descriptor (HOST struct) as cs_step does, without launching anything. */
+int cs_step_check(const cs_step_desc* d);
+
 /* Capture `steps` steps starting from buffer a into a CUDA graph (lbm.py:436-442); *graph receives an opaque
  * handle for cs_graph_launch / cs_graph_destroy. The stream must not be the legacy default stream. */
 int cs_graph_capture(const cs_step_desc* d, int32_t a, int32_t steps, void* stream, void** graph);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Batched step — many independent lattices (vessels of different sizes, clots and drives) advanced together. The
+ * reference runs one simulation per GPU process (a Slurm job array); here the instances' node lists are
+ * concatenated into one work list, and one persistent launch per kernel and step covers all of them: every block
+ * takes work items (a bulk block of some instance, or a boundary block) from the list and loads that instance's
+ * descriptor into shared memory. Each instance keeps its own buffers, clock, drive, outlet pressures and coupling.
+ * ------------------------------------------------------------------------------------------------------------- */
+typedef struct cs_batch_desc {
+    int32_t n_inst;
+    int32_t storage, model, gal, force; /* shared by all instances; force = some instance has a body force */
+    int32_t any_open;                   /* some instance has the resistance coupling (runs k_bc per instance) */
+    int32_t block;                      /* threads per bulk block, every instance (its flux_block must match) */
+    int32_t grid_bulk, grid_bnd;        /* persistent grid sizes; 0 = one block per work item */
+    int32_t bulk_items;                 /* sum over instances of ceil(n / block) */
+    int32_t bnd_items;                  /* sum over instances of 27 * max(1, ceil(gmax / 256)) */
+    const cs_step_desc* descs;          /* device array (n_inst), each checked with cs_step_check */
+    const int32_t* parity;              /* device (n_inst): instance i reads buffer a ^ parity[i] */
+    const int32_t* bulk_prefix;         /* device (n_inst + 1): first bulk work item of each instance */
+    const int32_t* bnd_prefix;          /* device (n_inst + 1): first boundary work item of each instance */
+} cs_batch_desc;
+
+/* Enqueue `steps` batched steps; the first reads buffer a ^ parity[i] of instance i. */
+int cs_batch_step(const cs_batch_desc* b, int32_t a, int32_t steps, void* stream);
+int cs_batch_graph_capture(const cs_batch_desc* b, int32_t a, int32_t steps, void* stream, void** graph);
 int cs_graph_launch(void* graph, void* stream);
 int cs_graph_destroy(void* graph);
 
@@ -215,7 +245,7 @@ int cs_last_error(char* buf, int32_t len);
 const char* cs_version(void);
 
 /* sizeof of the ABI structs, so that bindings can check their layout: which = 0 cs_opening, 1 cs_step_desc;
- * which = 2 returns CS_SEG_STRIDE. */
+ * which = 2 returns CS_SEG_STRIDE, 3 sizeof(cs_batch_desc). */
 size_t cs_abi_sizeof(int32_t which);
 
 #ifdef __cplusplus

@@ -1,0 +1,139 @@
+"""BatchSolver: several vessels in one persistent launch per step.
+
+- Alone and in the mix: an instance in a batch of its own and the same instance in a batch with other vessels
+  evolve bit for bit alike (same kernels, each instance on its own buffers, slab fluxes reduced in a fixed order
+  without atomics), whatever the mix and whenever instances join or leave.
+- Batched and dedicated kernels: the batched kernels and the single-lattice kernels are compiled separately and
+  may round differently in the last bit; they agree within the path's tolerance, relative L2 <= 1e-5.
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+from cerebrosim_b200 import lbm  # noqa: E402
+from cerebrosim_b200.batch import BatchSolver  # noqa: E402
+from cerebrosim_b200.simulate import ArterySolver  # noqa: E402
+
+
+def lattice(golden, name):
+    meta, arr = golden.small_case(name)
+    return lbm.build_lattice(arr["phi"], meta["origin"], meta["dx"], openings=meta["openings"],
+                             periodic=meta["periodic"], opening_slack=meta["slack"])
+
+
+def flux_for(lat):
+    z = lat["coords"][:, 2]
+    lo = np.flatnonzero((z >= 3) & (z < 5))
+    hi = np.flatnonzero((z >= z.max() - 5) & (z < z.max() - 3))
+    idx = np.concatenate([lo, hi])
+    slot = np.concatenate([np.zeros(len(lo), int), np.ones(len(hi), int)])
+    w = np.tile(np.array([[0.0, 0.0, 0.5]], np.float32), (len(idx), 1))
+    return {"idx": idx, "w": w, "slot": slot}
+
+
+SPECS = [("stenosis70_D8", dict(drive=([0.03], 1, 300), p=[0.0]), "plain"),
+         ("open_pipe_tilted_R4", dict(drive=([0.02, 0.004, -0.003], 250, 100), p=[1e-4]), "plain"),
+         ("box_openings_slack1", dict(drive=([0.01], 1, 100), p=[0.0, 2e-4, -1e-4]), "plain"),
+         ("open_pipe_straight_R4", dict(drive=([2e-4, 1e-4, 0.0], 300, 100), p=None), "artery")]
+
+
+def make(golden, name, cfg, kind, storage="f32"):
+    lat = lattice(golden, name)
+    if kind == "artery":
+        ops = [dict(o, kind="outlet") for o in lat["openings"]]
+        meta, arr = golden.small_case(name)
+        lat = lbm.build_lattice(arr["phi"], meta["origin"], meta["dx"], openings=ops)
+        s = ArterySolver(lat, 0.01, flux_for(lat), [0.0, 0.05], 1e-4, 0.01, model="regularised", storage=storage,
+                         block=256)
+        s.set_outlet_pressure([0.0, -1e-4])
+        s.set_sponge(4, 0.55, kinds=("outlet",))
+    else:
+        s = lbm.Solver(lat, 0.02, model="regularised", storage=storage, block=256)
+        s.set_sponge(4, 0.6)
+        s.set_outlet_pressure(cfg["p"])
+    coef, period, ramp = cfg["drive"]
+    s.set_drive(coef, period=period, ramp=ramp)
+    return s
+
+
+def same(a, b):
+    pa, ua = a.fields()
+    pb, ub = b.fields()
+    assert a.ok() and b.ok()
+    assert np.array_equal(pa, pb) and np.array_equal(ua, ub)
+    assert a.tick_value() == b.tick_value()
+    if isinstance(a, ArterySolver):
+        assert np.array_equal(a.Qlast.numpy(), b.Qlast.numpy())
+        assert np.array_equal(a.p_out.cpu().numpy(), b.p_out.cpu().numpy())
+
+
+def close(a, b, tol=1e-5):
+    pa, ua = a.fields()
+    pb, ub = b.fields()
+    assert a.ok() and b.ok()
+    e_u = np.sqrt(((ua - ub) ** 2).sum() / (ub ** 2).sum())
+    e_r = np.sqrt(((3 * pa.astype(np.float64) - 3 * pb) ** 2).sum() / ((1 + 3 * pb.astype(np.float64)) ** 2).sum())
+    assert e_u <= tol and e_r <= tol, (e_u, e_r)
+    assert a.tick_value() == b.tick_value()
+
+
+def run_alone(s, steps, chunk):
+    """An instance in a batch of its own."""
+    b = BatchSolver([s])
+    b.run(steps, chunk=chunk)
+    return b
+
+
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+def test_batch_alone_and_in_the_mix(golden, storage):
+    alone = [make(golden, n, c, k, storage) for n, c, k in SPECS]
+    mixed = [make(golden, n, c, k, storage) for n, c, k in SPECS]
+    for s in alone:
+        run_alone(s, 501, 100)
+    b = BatchSolver(mixed)
+    b.run(501, chunk=100)
+    assert b.steps == 501 and all(m.steps == 501 for m in mixed)
+    for a, m in zip(alone, mixed):
+        same(a, m)
+
+
+def test_batched_kernels_match_dedicated_kernels(golden):
+    dedicated = [make(golden, n, c, k) for n, c, k in SPECS]
+    batched = [make(golden, n, c, k) for n, c, k in SPECS]
+    for s in dedicated:
+        s.run(501, chunk=100)
+    BatchSolver(batched).run(501, chunk=100)
+    for a, m in zip(dedicated, batched):
+        close(a, m)
+
+
+def test_batch_members_join_and_leave(golden):
+    """Continuous batching: instances join with their own parity and step count and leave mid-run."""
+    alone = [make(golden, n, c, k) for n, c, k in SPECS]
+    mixed = [make(golden, n, c, k) for n, c, k in SPECS]
+    run_alone(mixed[1], 7, 40)                        # an odd head start: the member joins with parity 1
+    b = BatchSolver(mixed[:2])
+    b.run(100, chunk=40)
+    b.add(mixed[2])
+    b.run(130, chunk=40)
+    b.remove(mixed[0])
+    b.add(mixed[3])
+    b.run(61, chunk=40)
+    steps = [100 + 130, 7 + 100 + 130 + 61, 130 + 61, 61]
+    for s, k in zip(alone, steps):
+        run_alone(s, k, 40)
+    for a, m in zip(alone, mixed):
+        same(a, m)
+
+
+def test_coupled_runs_are_reproducible(golden):
+    """The resistance coupling reduces its flux without atomics: two runs agree bit for bit."""
+    n, c, k = SPECS[3]
+    r1, r2 = make(golden, n, c, k), make(golden, n, c, k)
+    for s in (r1, r2):
+        s.run(700, chunk=100)
+    same(r1, r2)
+    assert np.abs(r1.Qlast.numpy()).max() > 0
+    assert torch.equal(r1.f[r1.cur], r2.f[r2.cur])
