@@ -62,6 +62,8 @@ _I32, _I64, _D, _SZ = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_
 
 # name -> (restype, argtypes); every symbol declared in include/cerebrosim.h
 SIGNATURES = {
+    "cs_sdf_vessel": (_I32, [_P, _P, _P, _P, _I32, _P, _P, _P, ctypes.c_float, ctypes.POINTER(ctypes.c_float),
+                             ctypes.c_float, _I64, _I64, _I64, _P, _P]),
     "cs_lattice_scratch_bytes": (_SZ, [_I64, _I64, _I64]),
     "cs_lattice_count": (_I32, [_P, _I64, _I64, _I64, _P, ctypes.POINTER(_I64), _P]),
     "cs_lattice_fill": (_I32, [_P, _I64, _I64, _I64, ctypes.POINTER(_D), _D, ctypes.POINTER(Opening), _I32, _I32,

@@ -82,11 +82,17 @@ def build_lattice(phi, origin, dx, openings=(), periodic=(), opening_slack=1.0, 
     coords (N, 3) int32, origin, dx, shape, n_outlets, counts, openings), bit-identical to lbm.build_lattice, plus
     "_dev": the same tables as CUDA tensors, which `Solver` reuses instead of uploading them again."""
     lib = _lib.load()
-    dev = _device(device)
-    phi_h = np.ascontiguousarray(np.asarray(phi, np.float32))
-    if phi_h.ndim != 3:
-        raise ValueError(f"phi must be 3-D, got shape {phi_h.shape}")
-    nx, ny, nz = (int(s) for s in phi_h.shape)
+    if isinstance(phi, torch.Tensor) and phi.is_cuda:   # a field already on the device (vessel.sdf_grid)
+        dev = _device(phi.device if device is None else device)
+        phi_h = None
+        shape = tuple(int(s) for s in phi.shape)
+    else:
+        dev = _device(device)
+        phi_h = np.ascontiguousarray(np.asarray(phi, np.float32))
+        shape = phi_h.shape
+    if len(shape) != 3:
+        raise ValueError(f"phi must be 3-D, got shape {shape}")
+    nx, ny, nz = shape
     origin_a = np.asarray(origin, float)
     mask = 0
     for a in periodic:
@@ -109,7 +115,8 @@ def build_lattice(phi, origin, dx, openings=(), periodic=(), opening_slack=1.0, 
     with torch.cuda.device(dev):
         stream = torch.cuda.current_stream(dev)
         sp = ctypes.c_void_p(stream.cuda_stream)
-        phi_d = torch.from_numpy(phi_h).to(dev)
+        phi_d = (torch.from_numpy(phi_h).to(dev) if phi_h is not None
+                 else phi.to(dev, torch.float32).contiguous())
         scratch = torch.empty(max(1, int(lib.cs_lattice_scratch_bytes(nx, ny, nz))), dtype=torch.uint8, device=dev)
         n_fluid = ctypes.c_int64(0)
         check(lib.cs_lattice_count(ctypes.c_void_p(phi_d.data_ptr()), nx, ny, nz,
@@ -131,7 +138,7 @@ def build_lattice(phi, origin, dx, openings=(), periodic=(), opening_slack=1.0, 
         del scratch, phi_d
     cnt = counts.cpu().numpy()
     return {"nbr": nbr.cpu().numpy(), "q": q.cpu().numpy(), "uin": uin.cpu().numpy(), "coords": coords.cpu().numpy(),
-            "origin": origin_a, "dx": dx, "shape": phi_h.shape, "n_outlets": len(outlets),
+            "origin": origin_a, "dx": dx, "shape": shape, "n_outlets": len(outlets),
             "counts": {"wall": int(cnt[0]), "inlet": int(cnt[1]), "outlet": [int(x) for x in cnt[2:]]},
             "openings": inlets + outlets, "_dev": {"nbr": nbr, "q": q, "uin": uin, "coords": coords}}
 

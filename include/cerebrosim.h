@@ -58,6 +58,21 @@ typedef struct cs_opening {
 } cs_opening;
 
 /* ---------------------------------------------------------------------------------------------------------------
+ * Vessel signed distance — replaces vessel.k_sdf + vessel.sdf_grid (vessel.py:178-207, 230-245).
+ * ------------------------------------------------------------------------------------------------------------- */
+
+/* Signed distance (negative inside) of a branched vessel on the voxel centres origin + (i, j, k) dx, float32, C
+ * order (k fastest), written to out (nx * ny * nz floats), evaluated in float32 like vessel.k_sdf: per branch the
+ * minimum over its segments of the round-cone distance, cut by the flat caps within 2.5 cap radii of each open end,
+ * branches joined by the polynomial smooth minimum of radius blend. Centrelines are packed as vessel._packed
+ * (vessel.py:210-221) packs them: pts (n_pts * 3) and rad (n_pts) with the branches back to back, br_start /
+ * br_count (nbranch) per branch, cap_p / cap_n (2 nbranch * 3) and cap_r (2 nbranch, 0 = closed end) for the start
+ * and end of each branch. origin is a HOST pointer (3 floats); every other array is on the device. */
+int cs_sdf_vessel(const float* pts, const float* rad, const int32_t* br_start, const int32_t* br_count,
+                  int32_t nbranch, const float* cap_p, const float* cap_n, const float* cap_r, float blend,
+                  const float* origin, float dx, int64_t nx, int64_t ny, int64_t nz, float* out, void* stream);
+
+/* ---------------------------------------------------------------------------------------------------------------
  * Lattice / neighbour-table builder — replaces lbm.build_lattice (lbm.py:264-330), bit-exact tables.
  * Two phases because N is only known after the fluid count: cs_lattice_count, then cs_lattice_fill.
  * ------------------------------------------------------------------------------------------------------------- */

@@ -40,6 +40,7 @@ class Golden:
         self.hashes = json.load(open(os.path.join(GOLDEN, "tables_hash.json")))
         self.sponge = np.load(os.path.join(GOLDEN, "sponge.npz"))
         self.units = json.load(open(os.path.join(GOLDEN, "units.json")))
+        self.vessels = np.load(os.path.join(GOLDEN, "vessels.npz"))
 
     def small_names(self):
         return sorted({k.split("/")[0] for k in self.small.files})
@@ -48,6 +49,13 @@ class Golden:
         meta = json.loads(str(self.small[name + "/meta"]))
         arrays = {k: self.small[f"{name}/{k}"] for k in ("phi", "nbr", "q", "uin", "coords")}
         return meta, arrays
+
+    def vessel(self, case):
+        """The reference's packed centrelines of `case` (vessel._packed), its bounds and its openings."""
+        v = {k: self.vessels[f"{case}/{k}"] for k in ("pts", "rad", "start", "count", "cap_p", "cap_n", "cap_r",
+                                                       "lo", "hi")}
+        v["meta"] = json.loads(str(self.vessels[f"{case}/meta"]))
+        return v
 
 
 @pytest.fixture(scope="session")

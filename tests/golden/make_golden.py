@@ -242,6 +242,34 @@ def main(ref):
                           "WALL": lbm.WALL, "INLET": lbm.INLET, "OUTLET0": lbm.OUTLET0}
     with open(os.path.join(HERE, "units.json"), "w") as f:
         json.dump(units, f, indent=1)
+    # --- the reference's vessels (vessel.build is NumPy): centrelines, radii and caps as vessel.sdf_grid packs them
+    # (vessel.py:210-227), their bounds (vessel.py:224-227) and validate.artery_lattice's openings (validate.py:294-308)
+    import vessel as V
+    art = {}
+    for case in ("healthy", "narrow70", "occluded"):
+        g = V.build(case)
+        names, pts, rad, start, count, cp, cn, cr = V._packed(g)
+        lo, hi = V.bounds(g)
+        openings = []
+        for name, b in g["branches"].items():
+            for key, kind in (("start", "inlet"), ("end", "outlet")):
+                cap = b["caps"][key]
+                if cap is not None:
+                    r = b["R"][0] if key == "start" else b["R"][-1]
+                    openings.append({"kind": kind, "centre": np.asarray(cap[0], float).tolist(),
+                                     "normal": np.asarray(cap[1], float).tolist(), "radius": float(r)})
+        openings.sort(key=lambda o: o["kind"] != "inlet")
+        art[f"{case}/pts"] = pts
+        art[f"{case}/rad"] = rad
+        art[f"{case}/start"] = np.asarray(start, np.int32)
+        art[f"{case}/count"] = np.asarray(count, np.int32)
+        art[f"{case}/cap_p"] = cp
+        art[f"{case}/cap_n"] = cn
+        art[f"{case}/cap_r"] = cr
+        art[f"{case}/lo"] = np.asarray(lo, float)
+        art[f"{case}/hi"] = np.asarray(hi, float)
+        art[f"{case}/meta"] = np.array(json.dumps({"names": names, "blend": V.JUNCTION_BLEND, "openings": openings}))
+    np.savez_compressed(os.path.join(HERE, "vessels.npz"), **art)
     print("wrote", sorted(os.listdir(HERE)))
     for k, v in hashes.items():
         print(f"  {k}: N={v['N']} counts={v['counts']}")
