@@ -53,8 +53,11 @@ class BatchDesc(ctypes.Structure):
     _fields_ = [("n_inst", ctypes.c_int32), ("storage", ctypes.c_int32), ("model", ctypes.c_int32),
                 ("gal", ctypes.c_int32), ("force", ctypes.c_int32), ("any_open", ctypes.c_int32),
                 ("block", ctypes.c_int32), ("grid_bulk", ctypes.c_int32), ("grid_bnd", ctypes.c_int32),
-                ("bulk_items", ctypes.c_int32), ("bnd_items", ctypes.c_int32), ("descs", ctypes.c_void_p),
-                ("parity", ctypes.c_void_p), ("bulk_prefix", ctypes.c_void_p), ("bnd_prefix", ctypes.c_void_p)]
+                ("pad_", ctypes.c_int32), ("descs", ctypes.c_void_p), ("parity", ctypes.c_void_p),
+                ("counter", ctypes.c_void_p)]
+
+
+BATCH_GROUP = 64   # CS_BATCH_GROUP
 
 
 _P = ctypes.c_void_p

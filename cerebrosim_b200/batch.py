@@ -2,9 +2,10 @@
 
 The reference runs one simulation per GPU process and scales out with a Slurm job array of one-GPU jobs
 (slurm/submit_all.sh:21,36-38, slurm/config.sh:20); small vessels then leave most of a B200 idle. Here the
-instances' node lists are concatenated into one work list and a persistent kernel per step covers all of them
-(csrc/step.cu, `cs_batch_step`): each block takes work items — a bulk block or a boundary block of some instance —
-and reads that instance's descriptor (buffers, clock, drive, outlet pressures, coupling) into shared memory. The
+instances' node lists are concatenated into one work list and one persistent launch per kernel and step covers up
+to 64 of them (csrc/step.cu, `cs_batch_step`): each block takes work items — a bulk block or a boundary block of
+some instance — and reads that instance's descriptor (buffers, clock, drive, outlet pressures, coupling) from the
+kernel's parameters. The
 arithmetic of every instance is the single-lattice kernels' own, so an instance evolves exactly as it would alone.
 
 Instances may join and leave between runs (continuous batching): each keeps its own buffer parity, and the batch
@@ -12,14 +13,12 @@ descriptor table is rebuilt when the membership or an instance's parameters chan
 """
 import ctypes
 
-import numpy as np
 import torch
 
 from . import _lib
 from ._lib import check
 from .lbm import ctypes_void
 
-BOUNDARY_THREADS = 256
 
 
 class BatchSolver:
@@ -80,26 +79,19 @@ class BatchSolver:
         self.graphs = {}
 
     def _refresh(self):
-        """(Re)build the device descriptor table when members or their parameters changed."""
-        lib = _lib.load()
+        """(Re)build the batch descriptor when members or their parameters changed. The instances' descriptors
+        are host arrays the library copies into the kernels' parameters at every launch or capture."""
         descs = [m._desc() for m in self.members]
-        for d in descs:
-            check(lib.cs_step_check(ctypes.byref(d)))
         raw = b"".join(bytes(d) for d in descs)
         key = (raw, tuple(self._parity))
         if key == self._key:
             return
         self._drop_graphs()
         n = len(self.members)
-        bulk = [-(-m.N // self.block) if m.N else 0 for m in self.members]
-        bnd = [27 * max(1, -(-m.gmax // BOUNDARY_THREADS)) for m in self.members]
-        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
-            self._descs = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(self.dev)
-            self._par = torch.tensor(self._parity, dtype=torch.int32, device=self.dev)
-            self._bulk_prefix = torch.tensor(np.concatenate([[0], np.cumsum(bulk)]), dtype=torch.int32,
-                                             device=self.dev)
-            self._bnd_prefix = torch.tensor(np.concatenate([[0], np.cumsum(bnd)]), dtype=torch.int32,
-                                            device=self.dev)
+        self._descs = (_lib.StepDesc * n)(*descs)
+        self._par = (ctypes.c_int32 * n)(*self._parity)
+        with torch.cuda.device(self.dev):
+            self._counter = torch.zeros(-(-n // _lib.BATCH_GROUP), dtype=torch.int32, device=self.dev)
         m0 = self.members[0]
         b = _lib.BatchDesc()
         b.n_inst = n
@@ -107,12 +99,12 @@ class BatchSolver:
         b.force = int(any(any(x != 0.0 for x in m.force) for m in self.members))
         b.any_open = int(any(getattr(m, "n_open", 0) > 0 for m in self.members))
         b.block = self.block
-        b.bulk_items, b.bnd_items = int(sum(bulk)), int(sum(bnd))
         sms = torch.cuda.get_device_properties(self.dev).multi_processor_count
         b.grid_bulk = sms * 3 if self.persistent else 0          # 3 resident bulk blocks per SM
         b.grid_bnd = sms * 8 if self.persistent else 0           # 8 resident boundary blocks per SM
-        b.descs, b.parity = self._descs.data_ptr(), self._par.data_ptr()
-        b.bulk_prefix, b.bnd_prefix = self._bulk_prefix.data_ptr(), self._bnd_prefix.data_ptr()
+        b.descs = ctypes.addressof(self._descs)
+        b.parity = ctypes.addressof(self._par)
+        b.counter = self._counter.data_ptr()
         self.desc = b
         self._key = key
 

@@ -28,6 +28,8 @@
 
 #include "cs_common.cuh"
 
+#include <vector>
+
 namespace cs {
 namespace {
 
@@ -517,7 +519,6 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
 template <int ST, int MODEL, bool GAL, bool FORCE>
 __device__ __forceinline__ void bulk_body(const cs_step_desc& d, const int a, const int bx) {
     __shared__ float s_u[3][MAX_BLOCK];
-    __shared__ double s_q[MAX_OPEN];
     const int32_t n0 = int32_t(bx) * int32_t(blockDim.x);
     const int32_t n = n0 + int32_t(threadIdx.x);
     float ux = 0.f, uy = 0.f, uz = 0.f;
@@ -788,70 +789,109 @@ extern "C" int cs_graph_destroy(void* graph) {
 extern "C" int cs_step_check(const cs_step_desc* d) { return validate(d); }
 
 // ---- batched step -------------------------------------------------------------------------------------------------
+// The instances' descriptors travel in the kernels' parameter space (constant bank), CS_BATCH_GROUP instances per
+// launch: every block reads the descriptor of the instance it works on there, as the single-lattice kernels read
+// theirs, instead of staging it in shared memory (which costs registers and spills in the collision).
 namespace cs {
 namespace {
+
+struct BatchGroup {
+    int32_t n_inst, bulk_items, bnd_items, pad_;
+    int32_t* counter;
+    int32_t bulk_prefix[CS_BATCH_GROUP + 1];
+    int32_t bnd_prefix[CS_BATCH_GROUP + 1];
+    int32_t parity[CS_BATCH_GROUP];
+    cs_step_desc d[CS_BATCH_GROUP];
+};
+static_assert(sizeof(BatchGroup) < 32000, "batched kernel parameters exceed the 32 KB limit");
 
 // Largest i in [0, n) with prefix[i] <= item.
 __device__ __forceinline__ int find_instance(const int32_t* prefix, int n, int item) {
     int lo = 0, hi = n - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(prefix + mid) <= item) lo = mid; else hi = mid - 1;
+        if (prefix[mid] <= item) lo = mid; else hi = mid - 1;
     }
     return lo;
 }
 
-// The block's work item -> instance and local index, and the instance's descriptor copied to shared memory.
-__device__ __forceinline__ void take_item(const cs_batch_desc& b, const int32_t* prefix, int item, cs_step_desc& sd,
-                                          int& inst, int& local) {
-    __shared__ int s_inst, s_local;
-    if (threadIdx.x == 0) {
-        const int i = find_instance(prefix, b.n_inst, item);
-        s_inst = i;
-        s_local = item - __ldg(prefix + i);
+// A persistent block's share of the boundary work list: a contiguous range of items.
+struct ItemRange {
+    int lo, hi;
+    __device__ ItemRange(int items) {
+        const int per = items / int(gridDim.x), rem = items % int(gridDim.x), bx = int(blockIdx.x);
+        lo = bx * per + min(bx, rem);
+        hi = lo + per + (bx < rem ? 1 : 0);
     }
-    __syncthreads();
-    inst = s_inst;
-    local = s_local;
-    const int* src = reinterpret_cast<const int*>(b.descs + inst);
-    int* dst = reinterpret_cast<int*>(&sd);
-    for (int k = threadIdx.x; k < int(sizeof(cs_step_desc) / sizeof(int)); k += blockDim.x) dst[k] = __ldg(src + k);
-    __syncthreads();
-}
+};
+
+// Instance of each item for a block walking its items in increasing order.
+struct InstanceCursor {
+    const int32_t* prefix;
+    int n, inst = -1, first = 0, end = 0;
+    __device__ InstanceCursor(const int32_t* prefix_, int n_) : prefix(prefix_), n(n_) {}
+    __device__ __forceinline__ int next(int item) {
+        if (item >= end) {
+            inst = inst < 0 ? find_instance(prefix, n, item) : inst + 1;
+            while (prefix[inst + 1] <= item) ++inst;
+            first = prefix[inst];
+            end = prefix[inst + 1];
+        }
+        return item - first;
+    }
+};
 
 template <int ST>
-__global__ void __launch_bounds__(B_THREADS) k_boundary_batch(const cs_batch_desc b, const int a) {
-    __shared__ cs_step_desc sd;
-    for (int item = blockIdx.x; item < b.bnd_items; item += gridDim.x) {
-        int inst, local;
-        take_item(b, b.bnd_prefix, item, sd, inst, local);
-        const int nbx = int(max(int64_t(1), ceil_div(sd.gmax, B_THREADS)));
-        boundary_body<ST>(sd, a ^ __ldg(b.parity + inst), local % nbx, local / nbx);
-        __syncthreads();
+__global__ void __launch_bounds__(B_THREADS) k_boundary_batch(const __grid_constant__ BatchGroup g, const int a) {
+    const ItemRange r(g.bnd_items);
+    InstanceCursor cur(g.bnd_prefix, g.n_inst);
+    for (int item = r.lo; item < r.hi; ++item) {
+        const int local = cur.next(item);
+        const cs_step_desc& d = g.d[cur.inst];
+        const int nbx = int(max(int64_t(1), ceil_div(d.gmax, B_THREADS)));
+        boundary_body<ST>(d, a ^ g.parity[cur.inst], local % nbx, local / nbx);
+        __syncthreads();                        // boundary_body keeps the drive in shared memory
+    }
+    // the previous bulk kernel has finished (boundary_body waited for it) and the next one takes no item before
+    // this kernel ends: reset its work counter
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        grid_dependency_wait();
+        *g.counter = 0;
     }
 }
 
+// Bulk items are handed out dynamically: block x starts with item x, then takes the next unclaimed item from a
+// counter (reset by the boundary kernel each step), so that blocks finishing cheap items (few boundary rows) take
+// more of them. The claim for the following item is issued at the start of the current one and lands while it
+// runs. Which block updates which item does not change any result (each item writes its own nodes and its own row
+// of flux partial sums).
 template <int ST, int MODEL, bool GAL, bool FORCE>
-__global__ void __launch_bounds__(MAX_BLOCK, MIN_BLOCKS) k_bulk_batch(const cs_batch_desc b, const int a) {
-    __shared__ cs_step_desc sd;
-    for (int item = blockIdx.x; item < b.bulk_items; item += gridDim.x) {
-        int inst, local;
-        take_item(b, b.bulk_prefix, item, sd, inst, local);
-        bulk_body<ST, MODEL, GAL, FORCE>(sd, a ^ __ldg(b.parity + inst), local);
-        __syncthreads();
+__global__ void __launch_bounds__(MAX_BLOCK, MIN_BLOCKS) k_bulk_batch(const __grid_constant__ BatchGroup g,
+                                                                      const int a) {
+    __shared__ int s_item[2];
+    InstanceCursor cur(g.bulk_prefix, g.n_inst);
+    int item = blockIdx.x, buf = 0;
+    bool first = true;
+    while (item < g.bulk_items) {
+        const int local = cur.next(item);
+        int claim = 0;
+        if (!first && threadIdx.x == 0) claim = atomicAdd(g.counter, 1);
+        bulk_body<ST, MODEL, GAL, FORCE>(g.d[cur.inst], a ^ g.parity[cur.inst], local);
+        if (first && threadIdx.x == 0) claim = atomicAdd(g.counter, 1);   // after the wait inside bulk_body
+        first = false;
+        if (threadIdx.x == 0) s_item[buf] = int(gridDim.x) + claim;
+        __syncthreads();                        // also: the flux partial sums reuse shared memory
+        item = s_item[buf];
+        buf ^= 1;
     }
 }
 
-__global__ void k_bc_batch(const cs_batch_desc b) {
-    __shared__ cs_step_desc sd;
-    const int* src = reinterpret_cast<const int*>(b.descs + blockIdx.x);
-    int* dst = reinterpret_cast<int*>(&sd);
-    for (int k = threadIdx.x; k < int(sizeof(cs_step_desc) / sizeof(int)); k += blockDim.x) dst[k] = __ldg(src + k);
-    __syncthreads();
-    if (sd.n_open > 0) bc_body(sd);
+__global__ void k_bc_batch(const __grid_constant__ BatchGroup g) {
+    const cs_step_desc& d = g.d[blockIdx.x];
+    if (d.n_open > 0) bc_body(d);
 }
 
-using BatchFn = void (*)(const cs_batch_desc, const int);
+using BatchFn = void (*)(const BatchGroup, const int);
 
 template <int ST>
 BatchFn pick_batch_model(int model, int gal, bool force) {
@@ -865,18 +905,63 @@ BatchFn pick_batch_model(int model, int gal, bool force) {
 
 int validate_batch(const cs_batch_desc* b) {
     if (!b) return fail(CS_ERR_ARG, "cs_batch_step: null descriptor");
-    if (b->n_inst < 1 || !b->descs || !b->parity || !b->bulk_prefix || !b->bnd_prefix)
+    if (b->n_inst < 1 || !b->descs || !b->parity || !b->counter)
         return fail(CS_ERR_ARG, "cs_batch_step: %d instances or null tables", b->n_inst);
     if (b->storage < 0 || b->storage > 2 || (b->model != CS_MODEL_TRT && b->model != CS_MODEL_REGULARISED))
         return fail(CS_ERR_ARG, "cs_batch_step: storage %d model %d", b->storage, b->model);
     if (b->block < 32 || b->block > MAX_BLOCK || b->block % 32)
         return fail(CS_ERR_ARG, "cs_batch_step: block %d (32..%d, multiple of 32)", b->block, MAX_BLOCK);
-    if (b->bulk_items < 0 || b->bnd_items < b->n_inst * Q || b->grid_bulk < 0 || b->grid_bnd < 0)
-        return fail(CS_ERR_ARG, "cs_batch_step: work items %d / %d", b->bulk_items, b->bnd_items);
+    if (b->grid_bulk < 0 || b->grid_bnd < 0)
+        return fail(CS_ERR_ARG, "cs_batch_step: grid sizes %d / %d", b->grid_bulk, b->grid_bnd);
+    int64_t items = 0;
+    for (int i = 0; i < b->n_inst; ++i) {
+        const cs_step_desc& d = b->descs[i];
+        const int rc = validate(&d);
+        if (rc != CS_OK) return rc;
+        if (d.storage != b->storage || d.model != b->model || d.gal != b->gal || d.block != b->block)
+            return fail(CS_ERR_ARG, "cs_batch_step: instance %d differs from the batch in storage, model, Galilean "
+                                    "setting or block size", i);
+        if ((d.force[0] != 0.f || d.force[1] != 0.f || d.force[2] != 0.f) && !b->force)
+            return fail(CS_ERR_ARG, "cs_batch_step: instance %d has a body force but the batch has force = 0", i);
+        if (d.n_open > 0 && !b->any_open)
+            return fail(CS_ERR_ARG, "cs_batch_step: instance %d has open ends but the batch has any_open = 0", i);
+        if (b->parity[i] != 0 && b->parity[i] != 1)
+            return fail(CS_ERR_ARG, "cs_batch_step: parity[%d] = %d", i, b->parity[i]);
+        items += ceil_div(d.n, int64_t(b->block)) + int64_t(Q) * std::max(int64_t(1), ceil_div(d.gmax, int64_t(B_THREADS)));
+    }
+    if (items > INT32_MAX - int64_t(MAX_BLOCK) * 2048)
+        return fail(CS_ERR_SIZE, "cs_batch_step: %lld work items", (long long)items);
     return CS_OK;
 }
 
-int launch_batch_pdl(BatchFn fn, unsigned grid, unsigned block, cudaStream_t st, const cs_batch_desc& b, int a) {
+// The launch groups of a batch: CS_BATCH_GROUP instances each, work items counted per instance.
+std::vector<BatchGroup> make_groups(const cs_batch_desc* b) {
+    std::vector<BatchGroup> gs;
+    for (int i0 = 0; i0 < b->n_inst; i0 += CS_BATCH_GROUP) {
+        BatchGroup g;
+        std::memset(&g, 0, sizeof(g));
+        g.n_inst = std::min(CS_BATCH_GROUP, b->n_inst - i0);
+        g.counter = b->counter + i0 / CS_BATCH_GROUP;
+        int64_t bulk = 0, bnd = 0;
+        for (int k = 0; k < g.n_inst; ++k) {
+            const cs_step_desc& d = b->descs[i0 + k];
+            g.d[k] = d;
+            g.parity[k] = b->parity[i0 + k];
+            g.bulk_prefix[k] = int32_t(bulk);
+            g.bnd_prefix[k] = int32_t(bnd);
+            bulk += ceil_div(d.n, int64_t(b->block));
+            bnd += Q * std::max(int64_t(1), ceil_div(d.gmax, int64_t(B_THREADS)));
+        }
+        g.bulk_prefix[g.n_inst] = int32_t(bulk);
+        g.bnd_prefix[g.n_inst] = int32_t(bnd);
+        g.bulk_items = int32_t(bulk);
+        g.bnd_items = int32_t(bnd);
+        gs.push_back(g);
+    }
+    return gs;
+}
+
+int launch_batch_pdl(BatchFn fn, unsigned grid, unsigned block, cudaStream_t st, const BatchGroup& g, int a) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
@@ -886,12 +971,13 @@ int launch_batch_pdl(BatchFn fn, unsigned grid, unsigned block, cudaStream_t st,
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const cudaError_t e = cudaLaunchKernelEx(&cfg, fn, b, a);
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, fn, g, a);
     if (e != cudaSuccess) return fail(CS_ERR_CUDA, "launch of a batched step kernel failed: %s", cudaGetErrorString(e));
     return CS_OK;
 }
 
 int launch_batch(const cs_batch_desc* b, int a, int steps, cudaStream_t st) {
+    const std::vector<BatchGroup> gs = make_groups(b);
     const bool force = b->force != 0;
     BatchFn bulk = b->storage == CS_STORE_F16    ? pick_batch_model<CS_STORE_F16>(b->model, b->gal, force)
                    : b->storage == CS_STORE_BF16 ? pick_batch_model<CS_STORE_BF16>(b->model, b->gal, force)
@@ -899,18 +985,23 @@ int launch_batch(const cs_batch_desc* b, int a, int steps, cudaStream_t st) {
     BatchFn bound = b->storage == CS_STORE_F16    ? k_boundary_batch<CS_STORE_F16>
                     : b->storage == CS_STORE_BF16 ? k_boundary_batch<CS_STORE_BF16>
                                                   : k_boundary_batch<CS_STORE_F32>;
-    const unsigned gb = unsigned(b->grid_bnd > 0 ? std::min(b->grid_bnd, b->bnd_items) : b->bnd_items);
-    const unsigned gk = unsigned(b->grid_bulk > 0 ? std::min(b->grid_bulk, b->bulk_items) : b->bulk_items);
     for (int s = 0; s < steps; ++s) {
-        int rc = launch_batch_pdl(bound, gb, B_THREADS, st, *b, a);
-        if (rc != CS_OK) return rc;
-        if (gk > 0) {
-            rc = launch_batch_pdl(bulk, gk, unsigned(b->block), st, *b, a);
+        for (const BatchGroup& g : gs) {
+            const unsigned gb = unsigned(b->grid_bnd > 0 ? std::min(b->grid_bnd, g.bnd_items) : g.bnd_items);
+            const int rc = launch_batch_pdl(bound, gb, B_THREADS, st, g, a);
+            if (rc != CS_OK) return rc;
+        }
+        for (const BatchGroup& g : gs) {
+            const unsigned gk = unsigned(b->grid_bulk > 0 ? std::min(b->grid_bulk, g.bulk_items) : g.bulk_items);
+            if (gk == 0) continue;
+            const int rc = launch_batch_pdl(bulk, gk, unsigned(b->block), st, g, a);
             if (rc != CS_OK) return rc;
         }
         if (b->any_open) {
-            k_bc_batch<<<unsigned(b->n_inst), BC_THREADS, 0, st>>>(*b);
-            CS_CHECK_LAUNCH("k_bc_batch");
+            for (const BatchGroup& g : gs) {
+                k_bc_batch<<<unsigned(g.n_inst), BC_THREADS, 0, st>>>(g);
+                CS_CHECK_LAUNCH("k_bc_batch");
+            }
         }
         a = 1 - a;
     }

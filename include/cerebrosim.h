@@ -225,22 +225,25 @@ int cs_graph_capture(const cs_step_desc* d, int32_t a, int32_t steps, void* stre
 /* ---------------------------------------------------------------------------------------------------------------
  * Batched step — many independent lattices (vessels of different sizes, clots and drives) advanced together. The
  * reference runs one simulation per GPU process (a Slurm job array); here the instances' node lists are
- * concatenated into one work list, and one persistent launch per kernel and step covers all of them: every block
- * takes work items (a bulk block of some instance, or a boundary block) from the list and loads that instance's
- * descriptor into shared memory. Each instance keeps its own buffers, clock, drive, outlet pressures and coupling.
+ * concatenated into one work list, and one launch per kernel and step covers up to CS_BATCH_GROUP of them (larger
+ * batches launch one kernel per group): the blocks take work items (a bulk block of some instance, or a boundary
+ * block) from the list and read that instance's descriptor from the kernel's parameters. Each instance keeps its
+ * own buffers, clock, drive, outlet pressures and coupling.
  * ------------------------------------------------------------------------------------------------------------- */
+#define CS_BATCH_GROUP 64
+
 typedef struct cs_batch_desc {
     int32_t n_inst;
     int32_t storage, model, gal, force; /* shared by all instances; force = some instance has a body force */
     int32_t any_open;                   /* some instance has the resistance coupling (runs k_bc per instance) */
     int32_t block;                      /* threads per bulk block, every instance (its flux_block must match) */
     int32_t grid_bulk, grid_bnd;        /* persistent grid sizes; 0 = one block per work item */
-    int32_t bulk_items;                 /* sum over instances of ceil(n / block) */
-    int32_t bnd_items;                  /* sum over instances of 27 * max(1, ceil(gmax / 256)) */
-    const cs_step_desc* descs;          /* device array (n_inst), each checked with cs_step_check */
-    const int32_t* parity;              /* device (n_inst): instance i reads buffer a ^ parity[i] */
-    const int32_t* bulk_prefix;         /* device (n_inst + 1): first bulk work item of each instance */
-    const int32_t* bnd_prefix;          /* device (n_inst + 1): first boundary work item of each instance */
+    int32_t pad_;
+    const cs_step_desc* descs;          /* HOST array (n_inst); each is checked as cs_step_check does and copied
+                                           into the kernels' parameters at launch (a captured graph keeps its copy) */
+    const int32_t* parity;              /* HOST (n_inst): instance i reads buffer a ^ parity[i] */
+    int32_t* counter;                   /* DEVICE, ceil(n_inst / CS_BATCH_GROUP) ints, zero before the first step:
+                                           the bulk kernels' work counters (the boundary kernels reset them) */
 } cs_batch_desc;
 
 /* Enqueue `steps` batched steps; the first reads buffer a ^ parity[i] of instance i. */
