@@ -14,6 +14,14 @@ public API from host tables: Solver construction from pinned host arrays (H2D), 
 (D2H). Multi-GPU: independent replicas, one per rank, no collective on the data path ("scaling": "weak").
 --impl reference: the CPU restatement of the reference's step (oracle/, OpenMP on every host core) on the same
 workload, rank 0 only.
+
+At N = 1 the line also carries
+- "batched": the sweep of 16 generated stenosed arteries (0.3-3 M nodes each, 18.8 M in all) advanced together in
+  one batched launch per kernel and step, 16-bit shifted storage, --sweep-steps steps (one 8000-step beat), timed
+  with CUDA events; beside it the plain form: the same vessels one after another on dedicated FP32 solvers;
+- "served": the first --serve-requests requests of the seed-5 Poisson stream (2 per second) served with continuous
+  batching under a 150 GB budget (cerebrosim_b200.serve): per-beat latency p50 / p99, queue wait, aggregate MLUPS
+  over the makespan; beside it the same requests one by one in plain FP32, builds included in both.
 """
 import argparse
 import json
@@ -164,6 +172,86 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def bench_sweep(args, dev, peak):
+    """The batched sweep: 16 generated vessels (seeds 100-115, stenosis 0-100 %, 70-145 mmHg, 0.3-3 M nodes) in
+    one batched launch per kernel and step, 16-bit storage, against the plain form (each vessel alone, FP32)."""
+    import torch
+
+    from cerebrosim_b200 import workloads as W
+    from cerebrosim_b200.batch import BatchSolver
+
+    specs = W.sweep()
+    t0 = time.perf_counter()
+    lats = [W.spec_lattice(sp, device=dev)[1] for sp in specs]
+    build_s = time.perf_counter() - t0
+    steps = args.sweep_steps
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) * 1e-3
+
+    out = {"workload": "sweep of 16 generated stenosed arteries (seeds 100-115; stenosis 0, 10, ..., 90, 95, 100 % "
+                       "and 4 repeats; mean pressure 70-145 mmHg; 0.3-3 M nodes; tau 0.52; Fourier inflow, "
+                       "period 8000 steps)",
+           "instances": len(specs), "steps": steps, "build_s": build_s}
+    sol = [W.make_solver(sp, lat, storage=args.sweep_storage, device=dev) for sp, lat in zip(specs, lats)]
+    nodes = sum(x.N for x in sol)
+    b = BatchSolver(sol)
+    b.run(400, chunk=200)
+    clocks = Clocks(dev.index)
+    secs = timed(lambda: b.run(steps, chunk=200))
+    out["clocks"] = clocks.stop()
+    ok = all(x.ok() for x in sol)
+    mlups = nodes * steps / secs / 1e6
+    bplu = BPLU[args.sweep_storage]
+    out.update({"nodes": nodes, "storage": args.sweep_storage, "value": mlups, "unit": "MLUPS",
+                "hbm_gbs": bplu * mlups / 1e3, "frac": bplu * mlups / 1e3 / peak, "ok": ok,
+                "gpu_launches": 2 * steps, "seconds": secs})
+    del b, sol
+    # the plain form: each vessel on its own dedicated FP32 solver, one after another
+    tot = 0.0
+    ok = True
+    for sp, lat in zip(specs, lats):
+        x = W.make_solver(sp, lat, storage="f32", device=dev)
+        x.run(400, chunk=200)
+        tot += timed(lambda: x.run(steps, chunk=200))
+        ok &= x.ok()
+        del x
+    plain = nodes * steps / tot / 1e6
+    out["plain_f32_one_by_one"] = {"value": plain, "unit": "MLUPS", "hbm_gbs": BPLU["f32"] * plain / 1e3,
+                                   "frac": BPLU["f32"] * plain / 1e3 / peak, "ok": ok, "seconds": tot}
+    out["speedup_vs_plain"] = mlups / plain
+    return out
+
+
+def bench_served(args, dev):
+    """The served stream: Poisson arrivals (2/s, seed 5), clot U[0, 100] %, pressure U[70, 145] mmHg, 1-4 beats of
+    8000 steps, 0.2-4 M nodes, 150 GB budget, 16-bit storage; against the same requests one by one in plain FP32."""
+    from cerebrosim_b200 import serve, workloads as W
+
+    specs = W.request_stream(args.serve_requests, seed=5)
+    sv = serve.Server(budget_bytes=150e9, storage=args.sweep_storage, steps_per_beat=8000, chunk=1000,
+                      graph_chunk=200, device=dev, keep_fields=True)
+    clocks = Clocks(dev.index)
+    reqs = sv.serve(specs, realtime=True)
+    clk = clocks.stop()
+    st = serve.summary(reqs, 8000)
+    st["clocks"] = clk
+    st.update({"workload": f"first {len(specs)} requests of the seed-5 Poisson stream (2 requests/s)",
+               "storage": args.sweep_storage, "budget_gb": 150.0,
+               "max_active": max(n for _, n, _ in sv.trace),
+               "peak_reserved_gb": max(u for _, _, u in sv.trace) / 1e9})
+    plain = serve.one_by_one(specs, storage="f32", steps_per_beat=8000, device=dev)
+    st["plain_f32_one_by_one"] = plain
+    st["speedup_vs_plain"] = st["mlups"] / plain["mlups"]
+    return st
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -172,6 +260,9 @@ def main():
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sweep-steps", type=int, default=8000, help="steps of the batched sweep (0: skip it)")
+    ap.add_argument("--sweep-storage", default="bf16", choices=["f32", "f16", "bf16"])
+    ap.add_argument("--serve-requests", type=int, default=12, help="requests of the served stream (0: skip it)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -319,6 +410,10 @@ def main():
                 "whole_region_ms": whole0.elapsed_time(whole1)}
         if clk:
             line["clocks"] = clk
+        if world == 1 and args.sweep_steps > 0:
+            line["batched"] = bench_sweep(args, dev, peak)
+        if world == 1 and args.serve_requests > 0:
+            line["served"] = bench_served(args, dev)
         if world == 1 and not args.no_cpu_baseline:
             from oracle import lattice_ref as L
             line["cpu_baseline"] = cpu_baseline(plug_inlet(L.build_lattice(**cases.lattice_args(c))))

@@ -5,8 +5,8 @@ The reference runs one simulation per GPU process and scales out with a Slurm jo
 instances' node lists are concatenated into one work list and one persistent launch per kernel and step covers up
 to 64 of them (csrc/step.cu, `cs_batch_step`): each block takes work items — a bulk block or a boundary block of
 some instance — and reads that instance's descriptor (buffers, clock, drive, outlet pressures, coupling) from the
-kernel's parameters. The
-arithmetic of every instance is the single-lattice kernels' own, so an instance evolves exactly as it would alone.
+kernel's parameters. The arithmetic of every instance is the single-lattice kernels' own, so an instance evolves
+exactly as it would alone.
 
 Instances may join and leave between runs (continuous batching): each keeps its own buffer parity, and the batch
 descriptor table is rebuilt when the membership or an instance's parameters change.
@@ -19,6 +19,7 @@ from . import _lib
 from ._lib import check
 from .lbm import ctypes_void
 
+MAX_GROUPS = 64          # launch groups of CS_BATCH_GROUP instances: up to 4096 instances per batch
 
 
 class BatchSolver:
@@ -63,10 +64,14 @@ class BatchSolver:
         self._parity.append(s.cur ^ self.cur)
         self._key = None
 
-    def remove(self, s):
-        """Leave the batch; the instance keeps its state and can run alone or join another batch."""
+    def remove(self, s, sync=True):
+        """Leave the batch; the instance keeps its state and can run alone or join another batch.
+        sync=False returns at once: steps already enqueued still update the instance, so its buffers must stay
+        alive, and its fields are final only after the batch stream has passed them (a serving loop tracks that
+        with events)."""
         k = self.members.index(s)
-        self.stream.synchronize()
+        if sync:
+            self.stream.synchronize()
         del self.members[k]
         del self._parity[k]
         self._key = None
@@ -90,8 +95,12 @@ class BatchSolver:
         n = len(self.members)
         self._descs = (_lib.StepDesc * n)(*descs)
         self._par = (ctypes.c_int32 * n)(*self._parity)
-        with torch.cuda.device(self.dev):
-            self._counter = torch.zeros(-(-n // _lib.BATCH_GROUP), dtype=torch.int32, device=self.dev)
+        if n > MAX_GROUPS * _lib.BATCH_GROUP:
+            raise ValueError(f"{n} instances: at most {MAX_GROUPS * _lib.BATCH_GROUP} per batch")
+        if getattr(self, "_counter", None) is None:
+            # allocated once: graphs still in flight after a membership change keep using it
+            with torch.cuda.device(self.dev):
+                self._counter = torch.zeros(MAX_GROUPS, dtype=torch.int32, device=self.dev)
         m0 = self.members[0]
         b = _lib.BatchDesc()
         b.n_inst = n

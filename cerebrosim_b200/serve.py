@@ -1,0 +1,230 @@
+"""Serving loop: simulation requests (clot size, mean pressure, beats) solved as they arrive, with continuous batching.
+
+The reference runs each simulation as its own one-GPU job (simulate.py, submitted as a Slurm job array); a request
+waits for a whole GPU. Here one process serves a stream of requests on one GPU:
+
+- requests queue in arrival order; the head of the queue is admitted when the active set has a free slot and its
+  estimated device memory fits the HBM budget (its lattice is then built on the GPU and its populations stay
+  resident until its last beat);
+- every active request advances in the same batched launches (`BatchSolver`), chunk after chunk; a request joins
+  or leaves between chunks with its own buffer parity, so requests that arrive while others run overlap on the
+  device instead of waiting for them;
+- the host keeps `ahead` chunks enqueued and learns of their completion through CUDA events, so admissions, lattice
+  builds and result read-back overlap the GPU's work; beat ends are timed on the device timeline.
+
+Each request's result is the same as when it runs alone: the batched kernels apply each instance's own arithmetic
+to its own buffers, whatever else is in the launch.
+"""
+import collections
+import time
+
+import numpy as np
+import torch
+
+from . import workloads
+from .batch import BatchSolver
+
+# resident device bytes per fluid node, populations + velocity + tables (estimate used for admission; the
+# measured figure replaces it once the request is built)
+BYTES_PER_NODE = {"f32": 380.0, "f16": 270.0, "bf16": 270.0}
+
+
+class Request:
+    """One solve: `spec` as workloads.request_stream makes it ({id, arrival, seed, stenosis, pressure, beats,
+    nodes}). Filled in by the server: admit / done (seconds since the stream started), beat_end (device timeline,
+    seconds), queue_wait, N, bytes, ok, fields."""
+
+    def __init__(self, spec):
+        self.spec = dict(spec)
+        self.id = spec.get("id")
+        self.arrival = float(spec.get("arrival", 0.0))
+        self.beats = int(spec["beats"])
+        self.admit = None
+        self.done = None
+        self.beat_end = []
+        self.N = 0
+        self.bytes = 0
+        self.ok = None
+        self.fields = None
+        self.solver = None
+        self.steps_total = 0
+        self.steps_enq = 0
+
+    @property
+    def queue_wait(self):
+        return None if self.admit is None else self.admit - self.arrival
+
+    def beat_latencies(self):
+        """Wall time of each beat: from admission (first beat) or the previous beat's end to this beat's end."""
+        ends = [self.admit] + list(self.beat_end)
+        return [b - a for a, b in zip(ends[:-1], ends[1:])]
+
+
+def default_builder(spec, storage, block, device, steps_per_beat):
+    """Solver for a request: the workloads generator's vessel at the request's size, clot and pressure."""
+    g, lat, dx = workloads.spec_lattice(spec, device=device)
+    s = workloads.make_solver(spec, lat, storage=storage, block=block, period=steps_per_beat,
+                              ramp=min(1000, steps_per_beat // 8), device=device)
+    lat.pop("_dev", None)          # the full tables: the solver keeps its compressed form
+    for k in ("nbr", "q"):
+        lat.pop(k, None)
+    return s
+
+
+class Server:
+    """Continuous-batching server on one GPU.
+
+    budget_bytes: device memory the resident requests may hold (admission control); max_active: largest batch;
+    chunk: steps per scheduling round (a divisor of steps_per_beat); graph_chunk: steps per captured graph;
+    ahead: chunks kept enqueued; keep_fields: read each result's (p, u) back to the host."""
+
+    def __init__(self, budget_bytes=150e9, storage="bf16", steps_per_beat=8000, chunk=1000, graph_chunk=200,
+                 max_active=64, block=256, ahead=2, keep_fields=True, device=None, builder=default_builder):
+        if steps_per_beat % chunk or chunk % 2 or graph_chunk % 2:
+            raise ValueError("chunk must divide steps_per_beat; chunk and graph_chunk must be even")
+        self.budget = float(budget_bytes)
+        self.storage = storage
+        self.steps_per_beat = int(steps_per_beat)
+        self.chunk = int(chunk)
+        self.graph_chunk = int(min(graph_chunk, chunk))
+        self.max_active = int(max_active)
+        self.block = int(block)
+        self.ahead = max(1, int(ahead))
+        self.keep_fields = bool(keep_fields)
+        self.device = device
+        self.builder = builder
+        self.trace = []         # (seconds, active requests, reserved bytes) after each admission
+
+    def estimate(self, spec):
+        return BYTES_PER_NODE[self.storage] * float(spec["nodes"])
+
+    def _admit(self, r, batch, t0):
+        # built on the side stream, which never waits for the batch: the enqueued chunks keep running meanwhile
+        before = torch.cuda.memory_allocated(self.device)
+        with torch.cuda.stream(self._side):
+            s = self.builder(r.spec, self.storage, self.block, self.device, self.steps_per_beat)
+        self._side.synchronize()
+        s.synchronize()
+        r.bytes = max(0, torch.cuda.memory_allocated(self.device) - before)
+        r.solver, r.N = s, s.N
+        r.steps_total = r.beats * self.steps_per_beat
+        r.steps_enq = 0
+        batch.add(s)
+        r.admit = time.perf_counter() - t0
+
+    def _finish(self, r, t_done):
+        # the chunk that ended the request has completed: its buffers are final; read them on the side stream
+        s = r.solver
+        r.done = t_done
+        with torch.cuda.stream(self._side):
+            r.ok = s.ok()
+            if self.keep_fields:
+                r.fields = s.fields()
+        r.solver = None
+
+    def serve(self, specs, realtime=True):
+        """Serve the requests (arrival times in seconds from now when realtime, else all queued at once, in
+        arrival order) -> list of `Request` in arrival order, with timings and results."""
+        reqs = sorted((Request(s) for s in specs), key=lambda r: r.arrival)
+        if not realtime:
+            for r in reqs:
+                r.arrival = 0.0
+        self.trace = []
+        pending = collections.deque(reqs)
+        queue = collections.deque()
+        active = []
+        inflight = collections.deque()     # (event, [(request, steps enqueued after this chunk)])
+        used = 0.0
+        batch = None
+        self._side = torch.cuda.Stream(self.device)
+        t0 = time.perf_counter()
+        start = None
+        while pending or queue or active or inflight:
+            now = time.perf_counter() - t0
+            while pending and (not realtime or pending[0].arrival <= now):
+                queue.append(pending.popleft())
+            # admission: FIFO, while a slot is free and the estimate fits the budget
+            while queue and len(active) < self.max_active:
+                r = queue[0]
+                need = self.estimate(r.spec)
+                if used + need > self.budget:
+                    if not active and not inflight:
+                        raise RuntimeError(f"request {r.id} needs ~{need / 1e9:.1f} GB, over the "
+                                           f"{self.budget / 1e9:.1f} GB budget")
+                    break
+                queue.popleft()
+                if batch is None:
+                    batch = BatchSolver(block=self.block)
+                self._admit(r, batch, t0)
+                if start is None:
+                    start = torch.cuda.Event(enable_timing=True)
+                    start.record(batch.stream)
+                    base = time.perf_counter() - t0
+                used += max(need, r.bytes)
+                r.bytes_reserved = max(need, r.bytes)
+                active.append(r)
+                self.trace.append((r.admit, len(active), used))
+            if active:
+                batch.run(self.chunk, chunk=self.graph_chunk)
+                ev = torch.cuda.Event(enable_timing=True)
+                ev.record(batch.stream)
+                snap = []
+                for r in active:
+                    r.steps_enq += self.chunk
+                    snap.append((r, r.steps_enq))
+                inflight.append((ev, snap))
+                for r in [r for r in active if r.steps_enq >= r.steps_total]:
+                    batch.remove(r.solver, sync=False)
+                    active.remove(r)
+            # completed chunks: beat ends, finished requests (their buffers are final once the event has passed)
+            while inflight and (len(inflight) > self.ahead or not active or inflight[0][0].query()):
+                ev, snap = inflight.popleft()
+                ev.synchronize()
+                t = base + start.elapsed_time(ev) / 1e3
+                for r, steps in snap:
+                    if steps % self.steps_per_beat == 0:
+                        r.beat_end.append(t)
+                    if steps >= r.steps_total:
+                        self._finish(r, t)
+                        used -= r.bytes_reserved
+                if not active:
+                    break
+            if not active and not inflight and not queue and pending and realtime:
+                time.sleep(max(0.0, min(0.05, pending[0].arrival - (time.perf_counter() - t0))))
+        del batch
+        return reqs
+
+
+def summary(reqs, steps_per_beat):
+    """p50 / p99 of the per-beat latency and of the queue wait, and aggregate MLUPS over the whole stream."""
+    lat = np.array([x for r in reqs for x in r.beat_latencies()])
+    wait = np.array([r.queue_wait for r in reqs])
+    lu = sum(r.N * r.beats * steps_per_beat for r in reqs)
+    t_first = min(r.arrival for r in reqs)
+    t_last = max(r.done for r in reqs)
+    return {"requests": len(reqs), "beats": int(lat.size), "lattice_updates": float(lu),
+            "beat_latency_p50_s": float(np.percentile(lat, 50)), "beat_latency_p99_s": float(np.percentile(lat, 99)),
+            "queue_wait_p50_s": float(np.percentile(wait, 50)), "queue_wait_p99_s": float(np.percentile(wait, 99)),
+            "makespan_s": float(t_last - t_first), "mlups": float(lu / max(t_last - t_first, 1e-9) / 1e6),
+            "all_ok": bool(all(r.ok for r in reqs))}
+
+
+def one_by_one(specs, storage="f32", steps_per_beat=8000, graph_chunk=200, block=256, device=None,
+               builder=default_builder):
+    """The same requests run one after another, each on its own dedicated solver (plain form): total seconds,
+    lattice updates and MLUPS, builds included as in the served stream."""
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    lu = 0.0
+    ok = True
+    for sp in sorted(specs, key=lambda s: s.get("arrival", 0.0)):
+        s = builder(sp, storage, block, device, steps_per_beat)
+        steps = int(sp["beats"]) * steps_per_beat
+        s.run(steps, chunk=graph_chunk)
+        ok &= s.ok()
+        s.fields()
+        lu += s.N * steps
+        del s
+    torch.cuda.synchronize(device)
+    dt = time.perf_counter() - t0
+    return {"seconds": dt, "lattice_updates": lu, "mlups": lu / dt / 1e6, "all_ok": bool(ok)}

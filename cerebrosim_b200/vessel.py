@@ -114,12 +114,14 @@ def sdf_grid(g, dx, lo=None, hi=None, device=None, host=True):
 
 
 def openings_of(g):
-    """validate.py:297-305: an inlet at every capped branch start, an outlet at every capped end, inlets first."""
+    """validate.py:297-305: an inlet at every capped branch start, an outlet at every capped end, inlets first.
+    A cap given as (centre, normal, "closed") cuts the vessel flat like the others but is a wall, not an opening
+    (the faces of a clot that splits a vessel)."""
     ops = []
     for name, b in g["branches"].items():
         for key, kind in (("start", "inlet"), ("end", "outlet")):
             cap = b["caps"][key]
-            if cap is not None:
+            if cap is not None and not (len(cap) > 2 and cap[2] == "closed"):
                 r = b["R"][0] if key == "start" else b["R"][-1]
                 ops.append({"kind": kind, "centre": np.asarray(cap[0], float), "normal": np.asarray(cap[1], float),
                             "radius": float(r), "branch": name})

@@ -10,7 +10,8 @@ pressure need many vessels of controlled size, so this module generates them in 
   its start and a pressure outlet at its end;
 - a cosine stenosis of area reduction `stenosis` (0 .. 1) and length `sten_len` mm centred mid-parent: the radius
   is R (1 - delta (1 + cos(2 pi (s - s0) / sten_len)) / 2) within sten_len / 2 of the centre, (1 - delta)^2 =
-  1 - stenosis; a complete occlusion (stenosis 1) closes the lumen over the middle of the bump;
+  1 - stenosis; a complete occlusion (stenosis 1) is a solid clot `sten_len` long: the parent is split into a
+  proximal and a distal branch with flat closed faces at the clot;
 - a straight side branch of radius `branch_radius` leaving the parent at `branch_at` of its length (downstream of
   the stenosis) at `branch_angle` degrees to the parent's tangent, towards a seeded azimuth, `branch_len` mm long.
   Its far end is a pressure outlet, or, for an occluded parent, the velocity inlet: the occluded vessel is fed
@@ -57,11 +58,24 @@ def stenosed_vessel(seed=3, length=20.0, jitter=2.0, n_ctrl=5, radius=1.5, branc
     # cosine stenosis, centred mid-parent
     s0 = 0.5 * s[-1]
     w = np.where(np.abs(s - s0) < 0.5 * sten_len, 0.5 * (1 + np.cos(2 * np.pi * (s - s0) / sten_len)), 0.0)
-    delta = 1.25 if stenosis >= 1.0 else 1.0 - math.sqrt(1.0 - stenosis)   # 1.25: a solid plug mid-bump
+    delta = 1.0 - math.sqrt(max(0.0, 1.0 - stenosis))
     R0 = np.full(len(C), float(radius))
     R = R0 * (1.0 - delta * w)
     t0, t1 = _unit(C[1] - C[0]), _unit(C[-1] - C[-2])
-    trunk = {"C": C, "R0": R0, "R": R, "caps": {"start": (C[0].copy(), -t0), "end": (C[-1].copy(), t1)}}
+    branches = {}
+    if stenosis >= 1.0:
+        # occlusion: a solid clot sten_len long. A union of round cones cannot close a lumen over a bump shorter
+        # than its diameter, so the parent is split at the clot's faces, each face a flat closed cut
+        a_, b_ = np.searchsorted(s, s0 - 0.5 * sten_len), np.searchsorted(s, s0 + 0.5 * sten_len)
+        Cp, Cd = C[:a_], C[b_:]
+        tp, td = _unit(Cp[-1] - Cp[-2]), _unit(Cd[1] - Cd[0])
+        branches["trunk"] = {"C": Cp, "R0": R0[:a_], "R": R0[:a_].copy(),
+                             "caps": {"start": (Cp[0].copy(), -t0), "end": (Cp[-1].copy(), tp, "closed")}}
+        branches["trunk_distal"] = {"C": Cd, "R0": R0[b_:], "R": R0[b_:].copy(),
+                                    "caps": {"start": (Cd[0].copy(), -td, "closed"), "end": (Cd[-1].copy(), t1)}}
+    else:
+        branches["trunk"] = {"C": C, "R0": R0, "R": R,
+                             "caps": {"start": (C[0].copy(), -t0), "end": (C[-1].copy(), t1)}}
     # side branch from the parent's centreline at branch_at of its length
     k = int(np.argmin(np.abs(s - branch_at * s[-1])))
     tk = _unit(C[min(k + 1, len(C) - 1)] - C[max(k - 1, 0)])
@@ -72,9 +86,8 @@ def stenosed_vessel(seed=3, length=20.0, jitter=2.0, n_ctrl=5, radius=1.5, branc
     d = math.cos(th) * tk + math.sin(th) * (math.cos(a) * e1 + math.sin(a) * e2)
     Cb, _ = _resample(np.vstack([C[k], C[k] + branch_len * d]), spacing)
     Rb = np.full(len(Cb), float(branch_radius))
-    branch = {"C": Cb, "R0": Rb.copy(), "R": Rb, "caps": {"start": None, "end": (Cb[-1].copy(), d.copy())}}
-    return {"branches": {"trunk": trunk, "branch": branch},
-            "stenosis": float(stenosis), "seed": int(seed), "occluded": bool(stenosis >= 1.0)}
+    branches["branch"] = {"C": Cb, "R0": Rb.copy(), "R": Rb, "caps": {"start": None, "end": (Cb[-1].copy(), d.copy())}}
+    return {"branches": branches, "stenosis": float(stenosis), "seed": int(seed), "occluded": bool(stenosis >= 1.0)}
 
 
 def openings(g):

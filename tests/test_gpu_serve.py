@@ -1,0 +1,79 @@
+"""Serving loop: continuous batching with admission by an HBM budget, results alone and in the mix.
+
+- In the mix vs alone: each request served among others (joining and leaving the batch at different steps, with
+  other requests' vessels in the same launches) ends bit for bit where the same request ends when it is the only
+  one served: the batched kernels apply each instance's own arithmetic to its own buffers.
+- Against the dedicated single-lattice path: within relative L2 1e-5 of velocity and density (the batched and
+  single-lattice kernels are compiled separately and may round differently in the last bit).
+- Admission: the reserved memory never exceeds the budget; requests wait in the queue until memory frees up.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+from cerebrosim_b200 import serve, workloads  # noqa: E402
+
+SPB = 200           # steps per beat of the test workload
+
+
+def specs():
+    sizes = [30e3, 60e3, 20e3, 45e3, 25e3]
+    beats = [2, 1, 3, 1, 2]
+    sten = [0.3, 0.7, 0.0, 1.0, 0.5]
+    return [{"id": k, "arrival": 0.01 * k, "seed": 200 + k, "stenosis": sten[k], "pressure": 80.0 + 10 * k,
+             "beats": beats[k], "nodes": sizes[k]} for k in range(5)]
+
+
+def server(storage="bf16", **kw):
+    args = dict(storage=storage, steps_per_beat=SPB, chunk=50, graph_chunk=50, ahead=2)
+    args.update(kw)
+    return serve.Server(**args)
+
+
+def l2(a, b):
+    return float(np.sqrt(((a.astype(np.float64) - b) ** 2).sum() / max((b.astype(np.float64) ** 2).sum(), 1e-300)))
+
+
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+def test_served_results_same_alone_and_in_the_mix(storage):
+    sv = server(storage, max_active=3)
+    mix = sv.serve(specs(), realtime=False)
+    assert all(r.ok for r in mix)
+    # the mix really overlapped: up to three requests shared the launches, later ones joined mid-run
+    assert max(n for _, n, _ in sv.trace) == 3
+    assert max(r.queue_wait for r in mix) > 0
+    for r in mix:
+        assert len(r.beat_end) == r.beats and len(r.beat_latencies()) == r.beats
+        alone = server(storage).serve([r.spec], realtime=False)[0]
+        p0, u0 = alone.fields
+        p1, u1 = r.fields
+        assert np.array_equal(p0, p1) and np.array_equal(u0, u1), r.id
+
+
+def test_served_matches_dedicated_solver():
+    sp = specs()[0]
+    r = server("f32", max_active=3).serve(specs(), realtime=False)[0]
+    s = serve.default_builder(sp, "f32", 256, None, SPB)
+    s.run(sp["beats"] * SPB, chunk=50)
+    p, u = s.fields()
+    assert l2(r.fields[1], u) <= 1e-5 and l2(3 * r.fields[0] + 1, 3 * p + 1) <= 1e-5
+
+
+def test_admission_by_budget():
+    sv = server("bf16", budget_bytes=2.5 * serve.BYTES_PER_NODE["bf16"] * 60e3)
+    reqs = sv.serve(specs(), realtime=False)
+    assert all(r.ok for r in reqs)
+    assert all(used <= sv.budget for _, _, used in sv.trace)
+    # not everything fitted at once: some request waited for memory to free up
+    assert max(n for _, n, _ in sv.trace) < len(reqs)
+    assert max(r.queue_wait for r in reqs) > 0
+    st = serve.summary(reqs, SPB)
+    assert st["beats"] == sum(r.beats for r in reqs) and st["all_ok"]
+    assert st["beat_latency_p99_s"] >= st["beat_latency_p50_s"] > 0
+
+
+def test_request_over_budget_is_refused():
+    sv = server("bf16", budget_bytes=1e6)
+    with pytest.raises(RuntimeError, match="budget"):
+        sv.serve(specs()[:1], realtime=False)
