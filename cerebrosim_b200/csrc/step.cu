@@ -34,7 +34,7 @@ namespace cs {
 namespace {
 
 constexpr int MAX_BLOCK = 256;
-constexpr int MIN_BLOCKS = 3;   // 3 x 256 threads per SM: the register budget that keeps the pull unspilled
+constexpr int MIN_BLOCKS = 4;   // 4 x 256 threads per SM (64 registers): occupancy hides the pulls' latency
 constexpr int MAX_OPEN = 8;
 constexpr int B_THREADS = 256;
 constexpr float PI_F = 3.14159265358979323846f;
