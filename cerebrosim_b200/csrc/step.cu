@@ -221,6 +221,38 @@ __device__ __forceinline__ void boundary_body(const cs_step_desc& d, const int a
     const int32_t info = live ? __ldg(d.ginfo + slot) : 0;
     const float qslot = live ? __ldg(d.gq + slot) : 0.0f;
     grid_dependency_wait();
+    // issue the slot's loads first: the clock below (one thread, then a barrier) overlaps their latency
+    const int io = Lat::opp(i);
+    const float w = weight_rt(i), wo = weight_rt(io);
+    const uint32_t NP = uint32_t(d.npad);
+    const void* fin = d.f[a];
+    const bool live_node = node >= 0;
+    const uint32_t nn = live_node ? uint32_t(node) : 0u;
+    const bool is_wall = info >= CS_WALL, is_inlet = info == CS_INLET;
+    float fo = 0.0f, f2 = 0.0f, e0 = 0.0f, e1 = 0.0f, e2 = 0.0f, pk = 0.0f;
+    if (live_node) {
+        fo = Pop<ST>::ld(fin, uint32_t(io) * NP + nn, wo);
+        if (is_wall) {
+            if (d.bouzidi) {
+                if (qslot < 0.5f) {
+                    if (info >= 0) f2 = Pop<ST>::ld(fin, uint32_t(io) * NP + uint32_t(info), wo);
+                } else {
+                    f2 = Pop<ST>::ld(fin, uint32_t(i) * NP + nn, w);
+                }
+            }
+        } else if (is_inlet) {
+            const float* u = d.uin + 3 * int64_t(node);
+            e0 = __ldg(u);
+            e1 = __ldg(u + 1);
+            e2 = __ldg(u + 2);
+        } else {
+            const float* vin = d.vel[a];
+            e0 = __ldg(vin + node);
+            e1 = __ldg(vin + d.n + node);
+            e2 = __ldg(vin + 2 * d.n + node);
+            pk = __ldg(d.p_out + (CS_OUTLET0 - info));
+        }
+    }
     if (threadIdx.x == 0) {
         const int t = d.tick[a];
         s_drive = drive_value(d, t);
@@ -231,39 +263,30 @@ __device__ __forceinline__ void boundary_body(const cs_step_desc& d, const int a
     }
     __syncthreads();
     launch_dependents();                                    // the bulk kernel may start its static loads
-    if (node < 0) return;                                   // padding slot of a direction with fewer links
-    const int io = Lat::opp(i);
-    const float w = weight_rt(i), wo = weight_rt(io);
-    const uint32_t NP = uint32_t(d.npad);
-    const void* fin = d.f[a];
-    const float fo = Pop<ST>::ld(fin, uint32_t(io) * NP + uint32_t(node), wo);
+    if (!live_node) return;                                 // padding slot of a direction with fewer links
     const float cx = float(k_cx[i]), cy = float(k_cy[i]), cz = float(k_cz[i]);
     float v;
-    if (info >= CS_WALL) {
+    if (is_wall) {
         // lbm.py:163-173: interpolated bounce-back, or half-way bounce-back without Bouzidi
         v = fo;
         if (d.bouzidi) {
             const float q = qslot;
             if (q < 0.5f) {
-                if (info >= 0)
-                    v = 2.0f * q * fo + (1.0f - 2.0f * q) * Pop<ST>::ld(fin, uint32_t(io) * NP + uint32_t(info), wo);
+                if (info >= 0) v = 2.0f * q * fo + (1.0f - 2.0f * q) * f2;
             } else {
-                v = fo / (2.0f * q) + (2.0f * q - 1.0f) / (2.0f * q) * Pop<ST>::ld(fin, uint32_t(i) * NP + uint32_t(node), w);
+                v = fo / (2.0f * q) + (2.0f * q - 1.0f) / (2.0f * q) * f2;
             }
         }
-    } else if (info == CS_INLET) {
+    } else if (is_inlet) {
         // lbm.py:174-177: bounce-back with the prescribed velocity
-        const float* u = d.uin + 3 * int64_t(node);
         const float dv = s_drive;
-        const float cu = cx * (__ldg(u) * dv) + cy * (__ldg(u + 1) * dv) + cz * (__ldg(u + 2) * dv);
+        const float cu = cx * (e0 * dv) + cy * (e1 * dv) + cz * (e2 * dv);
         v = fo + 6.0f * w * cu;
     } else {
         // lbm.py:178-181: anti-bounce-back with the outlet's pressure and the previous velocity
-        const float* vin = d.vel[a];
-        const float ux = __ldg(vin + node), uy = __ldg(vin + d.n + node), uz = __ldg(vin + 2 * d.n + node);
-        const float cu = cx * ux + cy * uy + cz * uz;
-        const float usq = ux * ux + uy * uy + uz * uz;
-        v = -fo + 2.0f * w * (3.0f * __ldg(d.p_out + (CS_OUTLET0 - info)) + 4.5f * cu * cu - 1.5f * usq);
+        const float cu = cx * e0 + cy * e1 + cz * e2;
+        const float usq = e0 * e0 + e1 * e1 + e2 * e2;
+        v = -fo + 2.0f * w * (3.0f * pk + 4.5f * cu * cu - 1.5f * usq);
     }
     Pop<ST>::st(d.f[a], uint32_t(i) * NP + uint32_t(d.n + g), w, v);
 }
