@@ -1,9 +1,12 @@
 """Run a named lattice for a number of steps and print throughput (a small command-line front end).
 
     python -m cerebrosim_b200.run_case --case open_pipe_R24_L192 --steps 200 [--storage f16] [--block 128]
+    python -m cerebrosim_b200.run_case --artery 3 --steps 200 [--dx 0.05]    # a generated stenosed artery
 
 The open pipes get the pulsatile plug inlet used by bench.py (u0 (1 + 0.5 sin(2 pi t / 4000)), u0 = 0.02, tau 0.55,
-pressure outlet); periodic pipes get a body force. Steps run as CUDA graphs of 100 steps plus single launches.
+pressure outlet); periodic pipes get a body force. --artery SEED runs the stenosed-artery generator's vessel of that
+seed (70 % stenosis, side branch, Fourier inflow, tau 0.52; about 1.57 M nodes at dx 0.05 mm for seed 3). Steps run
+as CUDA graphs of 100 steps plus single launches.
 """
 import argparse
 import json
@@ -47,8 +50,17 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
     ap.add_argument("--block", type=int, default=None)
+    ap.add_argument("--artery", type=int, default=None, help="seed of a generated stenosed artery")
+    ap.add_argument("--dx", type=float, default=0.05, help="voxel size of --artery, mm")
     a = ap.parse_args()
-    s = make_solver(a.case, a.storage, a.block)
+    if a.artery is not None:
+        from . import workloads
+        spec = {"seed": a.artery, "stenosis": 0.7, "pressure": 95.0}
+        lat = workloads.lattice(workloads.stenosed_vessel(a.artery), a.dx)
+        s = workloads.make_solver(spec, lat, storage=a.storage, block=a.block or 256)
+        a.case = f"artery_seed{a.artery}_dx{a.dx}"
+    else:
+        s = make_solver(a.case, a.storage, a.block)
     s.run(10)
     s.synchronize()
     t = time.perf_counter()
