@@ -143,7 +143,6 @@ def cpu_baseline(lat, max_seconds=20.0):
 
 
 def run_reference(args):
-    import torch.distributed as dist  # noqa: F401
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -271,29 +270,17 @@ def main():
     import ctypes
 
     import torch
-    import torch.distributed as dist
-    from datetime import timedelta
 
     from cerebrosim_b200 import _lib, cases, lbm
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    from cerebrosim_b200.replicas import Replicas
+
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    rep = Replicas("nccl", timeout_s=120, device=dev)
+    world, rank = rep.world, rep.rank
+    barrier, max_over_ranks = rep.barrier, rep.max
 
     c = cases.case(WORKLOAD)
     lat = plug_inlet(lbm.build_lattice(**cases.lattice_args(c), device=dev))
@@ -418,8 +405,7 @@ def main():
             from oracle import lattice_ref as L
             line["cpu_baseline"] = cpu_baseline(plug_inlet(L.build_lattice(**cases.lattice_args(c))))
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    rep.close()
 
 
 if __name__ == "__main__":
