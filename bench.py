@@ -260,7 +260,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep-steps", type=int, default=8000, help="steps of the batched sweep (0: skip it)")
-    ap.add_argument("--sweep-storage", default="bf16", choices=["f32", "f16", "bf16"])
+    ap.add_argument("--sweep-storage", default="f16", choices=["f32", "f16", "bf16"])
     ap.add_argument("--serve-requests", type=int, default=12, help="requests of the served stream (0: skip it)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

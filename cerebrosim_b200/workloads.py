@@ -189,16 +189,22 @@ def spec_lattice(spec, device=None):
     return g, lattice(g, dx, device=device), dx
 
 
-def make_solver(spec, lat, tau=0.52, period=8000, ramp=1000, storage="f32", block=256, sponge=(8, 0.6),
-                device=None):
-    """Solver for a spec on its lattice: tau, a Fourier drive of period `period` steps scaled by the spec's
-    pressure, pressure outlets at 0, a sponge over `sponge[0]` cells at the openings."""
-    s = lbm.Solver(lat, (tau - 0.5) / 3.0, model="regularised", storage=storage, block=block, device=device)
+def configure(s, spec, lat, period=8000, ramp=1000, sponge=(8, 0.6)):
+    """A spec's boundary conditions on a solver (the package's or any with the reference's Solver interface): a
+    Fourier drive of period `period` steps scaled by the spec's pressure, pressure outlets at 0, a sponge over
+    `sponge[0]` cells at the openings."""
     s.set_sponge(sponge[0], sponge[1])
     s.set_outlet_pressure([0.0] * lat["n_outlets"])
     u = inflow_scale(spec["pressure"], spec["stenosis"])
     s.set_drive([c * u / 0.03 for c in fourier_drive(spec["seed"])], period=period, ramp=ramp)
     return s
+
+
+def make_solver(spec, lat, tau=0.52, period=8000, ramp=1000, storage="f32", block=256, sponge=(8, 0.6),
+                device=None):
+    """Solver for a spec on its lattice (tau, regularised collision), configured by `configure`."""
+    s = lbm.Solver(lat, (tau - 0.5) / 3.0, model="regularised", storage=storage, block=block, device=device)
+    return configure(s, spec, lat, period, ramp, sponge)
 
 
 def build_spec(spec, storage="f32", block=256, device=None, **kw):

@@ -253,6 +253,16 @@ int cs_graph_launch(void* graph, void* stream);
 int cs_graph_destroy(void* graph);
 
 /* ---------------------------------------------------------------------------------------------------------------
+ * Wall shear stress — replaces wss.shear (wss.py:50-57); the fit coefficients come from the host (wss.weights).
+ * ------------------------------------------------------------------------------------------------------------- */
+
+/* tau[v] = scale * sum_j c[v * K + j] (u_j - (u_j . n_v) n_v), u_j = U[idx[v * K + j]] (n_cells * 3 float, m/s),
+ * n_v = normals[v] (unit, into the lumen), accumulated in FP64; scale = mu * 1e3 for mm distances and Pa. Entries
+ * with c = 0 or an index outside 0 .. n_cells - 1 are skipped. Outputs tau (n_vert * 3 float). */
+int cs_wss_shear(const float* U, int64_t n_cells, const int32_t* idx, const float* c, const float* normals,
+                 int64_t n_vert, int32_t K, double scale, float* tau, void* stream);
+
+/* ---------------------------------------------------------------------------------------------------------------
  * Misc
  * ------------------------------------------------------------------------------------------------------------- */
 
