@@ -42,6 +42,7 @@ DRIVE = ([0.02, 0.0, 0.01], 4000)       # u0 (1 + 0.5 sin(2 pi t / T)): a0 = 0.0
 BPLU = {"f32": 356, "f16": 248, "bf16": 248}   # algorithmic bytes per lattice update
 METRIC = "D3Q27 MLUPS + HBM GB/s on 1 B200, plain vs batched/FP16; p50/p99 beat latency"
 FLUSH_BYTES = 256 << 20
+TUNED = {"block": 256, "order": "c"}     # launch shape of the batched / served forms (set by the sweep's autotuning)
 
 
 def nu_lu():
@@ -179,11 +180,19 @@ def bench_sweep(args, dev, peak):
     from cerebrosim_b200 import workloads as W
     from cerebrosim_b200.batch import BatchSolver
 
+    from cerebrosim_b200 import autotune
+
     specs = W.sweep()
     t0 = time.perf_counter()
     lats = [W.spec_lattice(sp, device=dev)[1] for sp in specs]
     build_s = time.perf_counter() - t0
     steps = args.sweep_steps
+    # block size and node order: tuned on the largest vessel, for its storage format, then used by every member
+    big = max(range(len(specs)), key=lambda k: lats[k]["nbr"].shape[1])
+    best, table = autotune.tune(lats[big], (0.52 - 0.5) / 3.0, storage=args.sweep_storage, steps=200, warmup=50,
+                                configure=lambda s: W.configure(s, specs[big], lats[big]), device=dev,
+                                model="regularised")
+    TUNED.update(block=best["block"], order=best["order"])
 
     def timed(fn):
         torch.cuda.synchronize()
@@ -197,10 +206,13 @@ def bench_sweep(args, dev, peak):
     out = {"workload": "sweep of 16 generated stenosed arteries (seeds 100-115; stenosis 0, 10, ..., 90, 95, 100 % "
                        "and 4 repeats; mean pressure 70-145 mmHg; 0.3-3 M nodes; tau 0.52; Fourier inflow, "
                        "period 8000 steps)",
-           "instances": len(specs), "steps": steps, "build_s": build_s}
-    sol = [W.make_solver(sp, lat, storage=args.sweep_storage, device=dev) for sp, lat in zip(specs, lats)]
+           "instances": len(specs), "steps": steps, "build_s": build_s,
+           "autotune": {"best": best, "candidates": table, "tuned_on": f"seed {specs[big]['seed']}, "
+                                                                         f"{lats[big]['nbr'].shape[1]} nodes"}}
+    sol = [W.make_solver(sp, lat, storage=args.sweep_storage, device=dev, block=best["block"], order=best["order"])
+           for sp, lat in zip(specs, lats)]
     nodes = sum(x.N for x in sol)
-    b = BatchSolver(sol)
+    b = BatchSolver(sol, block=best["block"])
     b.run(400, chunk=200)
     clocks = Clocks(dev.index)
     secs = timed(lambda: b.run(steps, chunk=200))
@@ -235,14 +247,14 @@ def bench_served(args, dev):
 
     specs = W.request_stream(args.serve_requests, seed=5)
     sv = serve.Server(budget_bytes=150e9, storage=args.sweep_storage, steps_per_beat=8000, chunk=1000,
-                      graph_chunk=200, device=dev, keep_fields=True)
+                      graph_chunk=200, device=dev, keep_fields=True, block=TUNED["block"], order=TUNED["order"])
     clocks = Clocks(dev.index)
     reqs = sv.serve(specs, realtime=True)
     clk = clocks.stop()
     st = serve.summary(reqs, 8000)
     st["clocks"] = clk
     st.update({"workload": f"first {len(specs)} requests of the seed-5 Poisson stream (2 requests/s)",
-               "storage": args.sweep_storage, "budget_gb": 150.0,
+               "storage": args.sweep_storage, "budget_gb": 150.0, "block": TUNED["block"], "order": TUNED["order"],
                "max_active": max(n for _, n, _ in sv.trace),
                "peak_reserved_gb": max(u for _, _, u in sv.trace) / 1e9})
     plain = serve.one_by_one(specs, storage="f32", steps_per_beat=8000, device=dev)

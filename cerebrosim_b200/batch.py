@@ -109,7 +109,8 @@ class BatchSolver:
         b.any_open = int(any(getattr(m, "n_open", 0) > 0 for m in self.members))
         b.block = self.block
         sms = torch.cuda.get_device_properties(self.dev).multi_processor_count
-        b.grid_bulk = sms * 3 if self.persistent else 0          # 3 resident bulk blocks per SM
+        # the bulk kernel keeps 1024 threads resident per SM (64 registers each): 4 blocks of 256, 8 of 128
+        b.grid_bulk = sms * max(1, 1024 // self.block) if self.persistent else 0
         b.grid_bnd = sms * 8 if self.persistent else 0           # 8 resident boundary blocks per SM
         b.descs = ctypes.addressof(self._descs)
         b.parity = ctypes.addressof(self._par)

@@ -187,14 +187,18 @@ class Solver:
     (magic = Lambda) or "regularised"; sigma < 1 blends the regularised stress with the finite-difference one.
 
     storage: "f32" (the reference's FP32 populations), "f16" or "bf16" (16-bit shifted populations, FP32
-    arithmetic). block: threads per block (None: the tuned default)."""
+    arithmetic). block: threads per block (None: the tuned default). order: internal node numbering ("c", the
+    lattice's own, or "axis" / "morton", see node_order); fields() always return the lattice's order, while the
+    state tensors (rho, vel, f) are in the internal one."""
 
     def __init__(self, lat, nu_lu, magic=3.0 / 16.0, bouzidi=True, model="trt", sigma=1.0, galilean=None,
-                 device=None, storage="f32", block=None):
+                 device=None, storage="f32", block=None, order="c"):
         lib = _lib.load()
         self.dev = _device(device)
         self.lat = lat
         self.N = N = int(lat["nbr"].shape[1])
+        perm = node_order(lat, order)
+        self.order = order
         self.tau = 3.0 * nu_lu + 0.5
         self.magic = float(magic)
         self.bouzidi = int(bool(bouzidi))
@@ -221,6 +225,16 @@ class Solver:
                     nbr = _upload(lat["nbr"], torch.int32, dev)
                     q = _upload(lat["q"], torch.float32, dev)
                     uin = _upload(lat["uin"], torch.float32, dev)
+                self.perm = self.inv = None
+                if perm is not None:
+                    # internal node k is the lattice's node perm[k]; sources renumbered through inv
+                    self.perm = torch.as_tensor(perm.astype(np.int64)).to(dev)
+                    self.inv = torch.empty_like(self.perm)
+                    self.inv[self.perm] = torch.arange(N, device=dev)
+                    src = nbr[:, self.perm]
+                    nbr = torch.where(src >= 0, self.inv[src.clamp(min=0)].to(torch.int32), src).contiguous()
+                    q = q[:, self.perm].contiguous()
+                    uin = uin[self.perm]
                 self.uin = uin.contiguous()
                 self.inl = (nbr == INLET).any(0).to(torch.int32) if N else torch.zeros(0, dtype=torch.int32, device=dev)
                 n_out = max(1, int(lat["n_outlets"]))
@@ -296,7 +310,10 @@ class Solver:
         tau = sponge_tau(self.lat, self.tau, length, tau_max, kinds)
         self.tau_cell = tau
         with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
-            self.om.copy_(torch.as_tensor((1.0 / tau).astype(np.float32)).to(self.dev) * self._om_sign)
+            om = torch.as_tensor((1.0 / tau).astype(np.float32)).to(self.dev)
+            if self.perm is not None:
+                om = om[self.perm]
+            self.om.copy_(om * self._om_sign)
 
     def set_outlet_pressure(self, p_lu):
         p = np.asarray(p_lu, np.float32).reshape(-1)
@@ -401,10 +418,15 @@ class Solver:
         return int(self.tick[self.cur].item())
 
     def fields(self):
-        """(pressure, velocity) per cell, lattice units, as NumPy (lbm.py:450-452)."""
+        """(pressure, velocity) per cell of the lattice (its node order, whatever the internal one), lattice units,
+        as NumPy (lbm.py:450-452)."""
         self.stream.synchronize()
-        rho = self.rho.cpu().numpy()
-        return rho / 3.0, np.ascontiguousarray(self.vel[self.cur].cpu().numpy().T)
+        rho, vel = self.rho, self.vel[self.cur]
+        if self.inv is not None:
+            with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+                rho, vel = rho[self.inv], vel[:, self.inv]
+            self.stream.synchronize()
+        return rho.cpu().numpy() / 3.0, np.ascontiguousarray(vel.cpu().numpy().T)
 
     def ok(self):
         """All densities finite (lbm.py:454-455)."""
@@ -416,6 +438,34 @@ class Solver:
             self._drop_graphs()
         except Exception:
             pass
+
+
+ORDERS = ("c", "axis", "morton")
+
+
+def node_order(lat, order="c"):
+    """Internal numbering of a lattice's nodes (internal node k = lattice node perm[k]); None for the lattice's own
+    C order. "axis": C order with the axis of largest extent varying fastest (long runs along a vessel); "morton":
+    Z-order curve of the grid coordinates."""
+    if order not in ORDERS:
+        raise ValueError(f"order {order!r}: one of {ORDERS}")
+    if order == "c" or lat["nbr"].shape[1] == 0:
+        return None
+    c = np.asarray(lat["coords"], np.int64)
+    if order == "axis":
+        ext = c.max(0) - c.min(0)
+        fast = int(np.argmax(ext))
+        slow = [a for a in (0, 1, 2) if a != fast]
+        perm = np.lexsort((c[:, fast], c[:, slow[1]], c[:, slow[0]]))
+    else:
+        code = np.zeros(len(c), np.int64)
+        for b in range(21):
+            for a in range(3):
+                code |= ((c[:, a] >> b) & 1) << (3 * b + (2 - a))
+        perm = np.argsort(code, kind="stable")
+    if np.array_equal(perm, np.arange(len(perm))):
+        return None
+    return perm
 
 
 def default_block(n):

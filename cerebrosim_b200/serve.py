@@ -60,11 +60,11 @@ class Request:
         return [b - a for a, b in zip(ends[:-1], ends[1:])]
 
 
-def default_builder(spec, storage, block, device, steps_per_beat):
+def default_builder(spec, storage, block, device, steps_per_beat, order="c"):
     """Solver for a request: the workloads generator's vessel at the request's size, clot and pressure."""
     g, lat, dx = workloads.spec_lattice(spec, device=device)
     s = workloads.make_solver(spec, lat, storage=storage, block=block, period=steps_per_beat,
-                              ramp=min(1000, steps_per_beat // 8), device=device)
+                              ramp=min(1000, steps_per_beat // 8), device=device, order=order)
     lat.pop("_dev", None)          # the full tables: the solver keeps its compressed form
     for k in ("nbr", "q"):
         lat.pop(k, None)
@@ -76,10 +76,12 @@ class Server:
 
     budget_bytes: device memory the resident requests may hold (admission control); max_active: largest batch;
     chunk: steps per scheduling round (a divisor of steps_per_beat); graph_chunk: steps per captured graph;
-    ahead: chunks kept enqueued; keep_fields: read each result's (p, u) back to the host."""
+    ahead: chunks kept enqueued; keep_fields: read each result's (p, u) back to the host; block and order: the
+    launch shape and node order of every request's solver (autotune.tune picks them)."""
 
     def __init__(self, budget_bytes=150e9, storage="bf16", steps_per_beat=8000, chunk=1000, graph_chunk=200,
-                 max_active=64, block=256, ahead=2, keep_fields=True, device=None, builder=default_builder):
+                 max_active=64, block=256, ahead=2, keep_fields=True, device=None, builder=default_builder,
+                 order="c"):
         if steps_per_beat % chunk or chunk % 2 or graph_chunk % 2:
             raise ValueError("chunk must divide steps_per_beat; chunk and graph_chunk must be even")
         self.budget = float(budget_bytes)
@@ -93,6 +95,7 @@ class Server:
         self.keep_fields = bool(keep_fields)
         self.device = device
         self.builder = builder
+        self.order = order
         self.trace = []         # (seconds, active requests, reserved bytes) after each admission
 
     def estimate(self, spec):
@@ -102,7 +105,7 @@ class Server:
         # built on the side stream, which never waits for the batch: the enqueued chunks keep running meanwhile
         before = torch.cuda.memory_allocated(self.device)
         with torch.cuda.stream(self._side):
-            s = self.builder(r.spec, self.storage, self.block, self.device, self.steps_per_beat)
+            s = self.builder(r.spec, self.storage, self.block, self.device, self.steps_per_beat, self.order)
         self._side.synchronize()
         s.synchronize()
         r.bytes = max(0, torch.cuda.memory_allocated(self.device) - before)
@@ -210,7 +213,7 @@ def summary(reqs, steps_per_beat):
 
 
 def one_by_one(specs, storage="f32", steps_per_beat=8000, graph_chunk=200, block=256, device=None,
-               builder=default_builder):
+               builder=default_builder, order="c"):
     """The same requests run one after another, each on its own dedicated solver (plain form): total seconds,
     lattice updates and MLUPS, builds included as in the served stream."""
     torch.cuda.synchronize(device)
@@ -218,7 +221,7 @@ def one_by_one(specs, storage="f32", steps_per_beat=8000, graph_chunk=200, block
     lu = 0.0
     ok = True
     for sp in sorted(specs, key=lambda s: s.get("arrival", 0.0)):
-        s = builder(sp, storage, block, device, steps_per_beat)
+        s = builder(sp, storage, block, device, steps_per_beat, order)
         steps = int(sp["beats"]) * steps_per_beat
         s.run(steps, chunk=graph_chunk)
         ok &= s.ok()

@@ -69,6 +69,8 @@ class ArterySolver(Solver):
             raise ValueError("flux idx outside the lattice")
         if len(slot) and (slot.min() < 0 or slot.max() >= n_open):
             raise ValueError("flux slot outside the open ends")
+        if self.inv is not None:                          # the lattice's node ids -> the internal numbering
+            idx = self.inv.cpu().numpy()[idx]
         order = np.argsort(idx, kind="stable")            # the fused reduction reads entries block by block
         dev = self.dev
         with torch.cuda.device(dev), torch.cuda.stream(self.stream):

@@ -201,9 +201,10 @@ def configure(s, spec, lat, period=8000, ramp=1000, sponge=(8, 0.6)):
 
 
 def make_solver(spec, lat, tau=0.52, period=8000, ramp=1000, storage="f32", block=256, sponge=(8, 0.6),
-                device=None):
+                device=None, order="c"):
     """Solver for a spec on its lattice (tau, regularised collision), configured by `configure`."""
-    s = lbm.Solver(lat, (tau - 0.5) / 3.0, model="regularised", storage=storage, block=block, device=device)
+    s = lbm.Solver(lat, (tau - 0.5) / 3.0, model="regularised", storage=storage, block=block, device=device,
+                   order=order)
     return configure(s, spec, lat, period, ramp, sponge)
 
 

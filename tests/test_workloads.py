@@ -74,3 +74,25 @@ def test_request_stream_and_sweep_specs():
     assert sorted(s["stenosis"] for s in sw[:12]) == [0.0, 0.1, 0.2, 0.3, 0.4, 0.5, 0.6, 0.7, 0.8, 0.9, 0.95, 1.0]
     assert np.isclose(min(s["nodes"] for s in sw), 0.3e6) and np.isclose(max(s["nodes"] for s in sw), 3e6)
     assert [s["pressure"] for s in sw] == [70.0 + 5 * k for k in range(16)]
+
+
+def test_node_orders_are_permutations():
+    from cerebrosim_b200 import lbm
+    rng = np.random.default_rng(1)
+    coords = np.unique(rng.integers(0, 40, size=(3000, 3)), axis=0)
+    coords = coords[np.lexsort((coords[:, 2], coords[:, 1], coords[:, 0]))]        # C order
+    lat = {"coords": coords, "nbr": np.zeros((27, len(coords)), np.int32)}
+    assert lbm.node_order(lat, "c") is None
+    for order in ("axis", "morton"):
+        perm = lbm.node_order(lat, order)
+        assert perm is None or np.array_equal(np.sort(perm), np.arange(len(coords)))
+    # a lattice longest along z is already in "axis" order
+    long_z = coords.copy()
+    long_z[:, 2] *= 10
+    assert lbm.node_order({"coords": long_z, "nbr": lat["nbr"]}, "axis") is None
+    # along x: the x coordinate varies fastest
+    long_x = coords[:, [2, 1, 0]] * np.array([10, 1, 1])
+    long_x = long_x[np.lexsort((long_x[:, 2], long_x[:, 1], long_x[:, 0]))]
+    perm = lbm.node_order({"coords": long_x, "nbr": lat["nbr"]}, "axis")
+    c = long_x[perm]
+    assert np.all(np.diff(c[:, 0])[(np.diff(c[:, 2]) == 0) & (np.diff(c[:, 1]) == 0)] > 0)
