@@ -8,7 +8,9 @@ on the CPU oracle (oracle/lbm_ref.cpp, the same scheme in double). Compared at t
 - wall shear stress: at the wall points of the lattice's wall links, by the weighted near-wall fit (wss.py:35-57;
   the same fit coefficients for every run), relative L2 of the shear vectors and relative error of the mean
   magnitude.
-The voxel size and beats can be raised with CS_PRECISION_DX (mm) and CS_PRECISION_BEATS.
+The voxel size and beats can be raised with CS_PRECISION_DX (mm) and CS_PRECISION_BEATS; the bounds below hold at
+the default 0.2 mm. At finer voxels the flow per cell is slower relative to the stored deviations and BF16's 8-bit
+mantissa falls behind (see the recorded study); FP16 holds velocity and WSS within 1 %.
 """
 import json
 import os
@@ -67,9 +69,11 @@ def test_storage_error_vs_fp64_oracle():
         s.run(steps, chunk=1000)
         assert s.ok()
         p, u = s.fields()
-        r = metrics(p.astype(float), u.astype(float), ref_p, ref_u, inlet, outlet, shear, tau_ref)
-        report[st] = r
+        report[st] = metrics(p.astype(float), u.astype(float), ref_p, ref_u, inlet, outlet, shear, tau_ref)
+    print("PRECISION", json.dumps(report))
+    for st, r in report.items():
+        if st not in LIMITS:
+            continue
         lim = LIMITS[st]
         assert r["velocity_rel_l2"] <= lim and r["pressure_drop_rel"] <= DP_LIMITS[st], (st, r)
         assert r["wss_rel_l2"] <= lim and r["wss_mean_rel"] <= lim, (st, r)
-    print("PRECISION", json.dumps(report))
