@@ -206,6 +206,111 @@ __device__ __forceinline__ float cdot(float ax, float ay, float az) {
     return s;
 }
 
+// The links the grouped sums below name by index: axis 1, 3, 5 (+x, +y, +z); edges 7 (1,1,0), 9 (1,-1,0), 11 (1,0,1),
+// 13 (1,0,-1), 15 (0,1,1), 17 (0,1,-1); corners 19 (1,1,1), 21 (1,1,-1), 23 (1,-1,1), 25 (-1,1,1); each with its
+// opposite at index + 1.
+constexpr bool pair_is(int i, int x, int y, int z) {
+    return Lat::cx(i) == x && Lat::cy(i) == y && Lat::cz(i) == z && Lat::opp(i) == i + 1;
+}
+static_assert(pair_is(1, 1, 0, 0) && pair_is(3, 0, 1, 0) && pair_is(5, 0, 0, 1), "axis links");
+static_assert(pair_is(7, 1, 1, 0) && pair_is(9, 1, -1, 0) && pair_is(11, 1, 0, 1) && pair_is(13, 1, 0, -1) &&
+                  pair_is(15, 0, 1, 1) && pair_is(17, 0, 1, -1), "edge links");
+static_assert(pair_is(19, 1, 1, 1) && pair_is(21, 1, 1, -1) && pair_is(23, 1, -1, 1) && pair_is(25, -1, 1, 1),
+              "corner links");
+
+// Moments of the 27 pulled values (dr = sum f, j = sum c f, Pi = sum c c^T f): each pair (I, opp I) enters through
+// its sum s and difference d, and the terms several moments share are added once — the three edge planes, and the
+// four corner pairs through a butterfly (their sums give the trace and the three off-diagonals of Pi, their
+// differences the corner parts of j). 81 additions instead of 111 for the link-by-link sums.
+__device__ __forceinline__ void moments27(const float (&f)[Q], Moments& m) {
+    float sp[Q / 2 + 1], dp[Q / 2 + 1];
+#pragma unroll
+    for (int k = 0; k < 13; ++k) {
+        sp[k] = f[1 + 2 * k] + f[2 + 2 * k];
+        dp[k] = f[1 + 2 * k] - f[2 + 2 * k];
+    }
+    // pair k holds links 1 + 2k and 2 + 2k: k = 0, 1, 2 axis; 3 .. 8 edges; 9 .. 12 corners
+    const float exy = sp[3] + sp[4], exz = sp[5] + sp[6], eyz = sp[7] + sp[8];
+    const float ca = sp[9] + sp[10], cb = sp[9] - sp[10], cc = sp[11] + sp[12], ce = sp[11] - sp[12];
+    const float sc = ca + cc;
+    m.dr = f[0] + sp[0] + sp[1] + sp[2] + exy + exz + eyz + sc;
+    m.pxx = sp[0] + exy + exz + sc;
+    m.pyy = sp[1] + exy + eyz + sc;
+    m.pzz = sp[2] + exz + eyz + sc;
+    m.pxy = (sp[3] - sp[4]) + (ca - cc);
+    m.pxz = (sp[5] - sp[6]) + (cb + ce);
+    m.pyz = (sp[7] - sp[8]) + (cb - ce);
+    const float dpp = dp[9] + dp[10], dpr = dp[9] - dp[10], dpt = dp[11] + dp[12], dpv = dp[11] - dp[12];
+    m.jx = dp[0] + dp[3] + dp[4] + dp[5] + dp[6] + (dpp + dpv);
+    m.jy = dp[1] + dp[3] - dp[4] + dp[7] + dp[8] + (dpp - dpv);
+    m.jz = dp[2] + dp[5] - dp[6] + dp[7] - dp[8] + (dpr + dpt);
+}
+
+// One pair's outputs w (A + e +- o) (the weight is the pair's).
+template <int ST, int I>
+__device__ __forceinline__ void store_pair(void* fout, uint32_t NP, int32_t n, float A, float e, float o) {
+    constexpr int O = Lat::opp(I);
+    constexpr float w = wgt(I);
+    const float wb = w * (A + e);
+    Pop<ST>::st(fout, uint32_t(I) * NP + uint32_t(n), w, fmaf(w, o, wb));
+    Pop<ST>::st(fout, uint32_t(O) * NP + uint32_t(n), w, fmaf(-w, o, wb));
+}
+
+// Regularised collision output without a body force (lbm.py:129-137, 230-240): f_I = w_I (A + e_I + o_I) and
+// f_opp = w_I (A + e_I - o_I), with e_I = c_I^T M c_I for M = 4.5 u u^T + 4.5 (1 - om) P' (given as its diagonal
+// and twice its off-diagonal: m*) and o_I = 3 c_I . u + h3_I (the third-order term, with the Galilean model). Axis,
+// edge and corner links differ only in signs, so the 13 pairs' e and o come from shared partial sums.
+template <int ST, bool GAL>
+__device__ __forceinline__ void store_regularised(void* fout, uint32_t NP, int32_t n, float A, float ux, float uy,
+                                                  float uz, float mxx, float myy, float mzz, float mxy2,
+                                                  float mxz2, float myz2) {
+    Pop<ST>::st(fout, uint32_t(n), wgt(0), wgt(0) * A);
+    // third-order terms from the velocity monomials: axis links -4.5 (sum of two), edges 9 (..) - 4.5 (..),
+    // corners 9 (+-A1 +-A2 +-A3) +- 27 xyz
+    float h1 = 0.f, h3 = 0.f, h5 = 0.f, h7 = 0.f, h9 = 0.f, h11 = 0.f, h13 = 0.f, h15 = 0.f, h17 = 0.f;
+    float h19 = 0.f, h21 = 0.f, h23 = 0.f, h25 = 0.f;
+    if (GAL) {
+        const float x2 = ux * ux, y2 = uy * uy, z2 = uz * uz;
+        const float xxy = x2 * uy, xxz = x2 * uz, xyy = ux * y2, yyz = y2 * uz, xzz = ux * z2, yzz = uy * z2;
+        const float xyz = ux * uy * uz;
+        const float a1 = xxy + yzz, a2 = xxz + yyz, a3 = xyy + xzz;
+        h1 = -4.5f * a3;
+        h3 = -4.5f * a1;
+        h5 = -4.5f * a2;
+        h7 = 9.0f * (xyy + xxy) - 4.5f * (xzz + yzz);
+        h9 = 9.0f * (xyy - xxy) - 4.5f * (xzz - yzz);
+        h11 = 9.0f * (xzz + xxz) - 4.5f * (xyy + yyz);
+        h13 = 9.0f * (xzz - xxz) - 4.5f * (xyy - yyz);
+        h15 = 9.0f * (yzz + yyz) - 4.5f * (xxy + xxz);
+        h17 = 9.0f * (yzz - yyz) - 4.5f * (xxy - xxz);
+        const float b1 = 9.0f * a1, b2 = 9.0f * a2, b3 = 9.0f * a3, bx = 27.0f * xyz;
+        const float p_ = b1 + b3, q_ = b2 + bx, m_ = b3 - b1, n_ = b2 - bx;
+        h19 = p_ + q_;
+        h21 = p_ - q_;
+        h23 = m_ + n_;
+        h25 = n_ - m_;
+    }
+    // axis
+    store_pair<ST, 1>(fout, NP, n, A, mxx, 3.0f * ux + h1);
+    store_pair<ST, 3>(fout, NP, n, A, myy, 3.0f * uy + h3);
+    store_pair<ST, 5>(fout, NP, n, A, mzz, 3.0f * uz + h5);
+    // edges, plane by plane
+    const float sxy = mxx + myy, sxz = mxx + mzz, syz = myy + mzz;
+    const float u7 = ux + uy, u9 = ux - uy;
+    store_pair<ST, 7>(fout, NP, n, A, sxy + mxy2, 3.0f * u7 + h7);
+    store_pair<ST, 9>(fout, NP, n, A, sxy - mxy2, 3.0f * u9 + h9);
+    store_pair<ST, 11>(fout, NP, n, A, sxz + mxz2, 3.0f * (ux + uz) + h11);
+    store_pair<ST, 13>(fout, NP, n, A, sxz - mxz2, 3.0f * (ux - uz) + h13);
+    store_pair<ST, 15>(fout, NP, n, A, syz + myz2, 3.0f * (uy + uz) + h15);
+    store_pair<ST, 17>(fout, NP, n, A, syz - myz2, 3.0f * (uy - uz) + h17);
+    // corners
+    const float tr = sxy + mzz, ca = tr + mxy2, cb = tr - mxy2, cg = mxz2 + myz2, cd = mxz2 - myz2;
+    store_pair<ST, 19>(fout, NP, n, A, ca + cg, 3.0f * (u7 + uz) + h19);
+    store_pair<ST, 21>(fout, NP, n, A, ca - cg, 3.0f * (u7 - uz) + h21);
+    store_pair<ST, 23>(fout, NP, n, A, cb + cd, 3.0f * (u9 + uz) + h23);
+    store_pair<ST, 25>(fout, NP, n, A, cb - cd, 3.0f * (uz - u9) + h25);
+}
+
 // ---- 1. boundary-link kernel and clock ----------------------------------------------------------------------------
 // Block (bx, by) of a lattice's boundary-link grid: by = direction, bx = chunk of its ghost slots. Called by every
 // thread of the block (it synchronises the block once).
@@ -353,24 +458,14 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
         for (int k = 0; k < 6; ++k) g[k] = __ldg(grad_src(d, vin, 1 + k, k / 2, lk[1 + k]));
     }
 
-    // TRT needs f_i and f_opp(i); the body-force path keeps the populations for the per-link evaluation below
-    constexpr bool KEEP = MODEL == CS_MODEL_TRT || FORCE;
+    // the 27 pulls (TRT and the body-force path use the populations themselves after the moments)
     Moments m;
-    float fk[KEEP ? Q : 1];
-    const float v0 = Pop<ST>::ld(fin, uint32_t(lk[0]), wgt(0));
-    m.dr = v0;
-    if constexpr (KEEP) fk[0] = v0;
-    Unroll<0, 13>::run([&](auto pc) {
-        constexpr int I = 1 + 2 * decltype(pc)::value;
-        constexpr int O = Lat::opp(I);
-        const float v = Pop<ST>::ld(fin, uint32_t(I) * NP + uint32_t(lk[I]), wgt(I));
-        const float vo = Pop<ST>::ld(fin, uint32_t(O) * NP + uint32_t(lk[O]), wgt(O));
-        m.add_pair<I>(v, vo);
-        if constexpr (KEEP) {
-            fk[I] = v;
-            fk[O] = vo;
-        }
+    float fk[Q];
+    Unroll<0, Q>::run([&](auto ic) {
+        constexpr int I = decltype(ic)::value;
+        fk[I] = Pop<ST>::ld(fin, uint32_t(I) * NP + uint32_t(lk[I]), wgt(I));
     });
+    moments27(fk, m);
 
     const bool inlet_cell = om_signed < 0.0f;
     const float om = fabsf(om_signed);
@@ -493,19 +588,12 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
         }
         // without a force: f_out = feq + (1 - om) fneq + (1 - om/2) src (lbm.py:236-240) regrouped as
         // w (A + E +- O), each pair's terms evaluated once
-        const float A = dr - 1.5f * usq - 4.5f * k_ne * trp - 3.0f * k_src * uF;
+        const float A = dr - 1.5f * usq - 4.5f * k_ne * trp;
         const float s = 4.5f * k_ne;
-        const float qxx = s * pxx, qyy = s * pyy, qzz = s * pzz;
-        const float qxy = 2.0f * s * pxy, qxz = 2.0f * s * pxz, qyz = 2.0f * s * pyz;
-        const float ka = 3.0f * k_src - 1.5f * k_ne, kb = 9.0f * k_src;
-        const float fax = ka * Fx, fay = ka * Fy, faz = ka * Fz;
-        const float fbx = kb * Fx, fby = kb * Fy, fbz = kb * Fz;
-        store_pairs<ST>(fout, NP, n, A, [&](auto ic, float& e, float& o) {
-            constexpr int I = decltype(ic)::value;
-            const float cu = cdot<I>(ux, uy, uz);
-            e = cu * (4.5f * cu + cdot<I>(fbx, fby, fbz)) + quad<I>(qxx, qyy, qzz, qxy, qxz, qyz);
-            o = 3.0f * cu + cdot<I>(fax, fay, faz) + t3 * cu3.template h3<I>();
-        });
+        const float hx = 4.5f * ux, hy = 4.5f * uy;
+        store_regularised<ST, GAL>(fout, NP, n, A, ux, uy, uz, fmaf(hx, ux, s * pxx), fmaf(hy, uy, s * pyy),
+                                   fmaf(4.5f * uz, uz, s * pzz), fmaf(2.0f * hx, uy, 2.0f * s * pxy),
+                                   fmaf(2.0f * hx, uz, 2.0f * s * pxz), fmaf(2.0f * hy, uz, 2.0f * s * pyz));
     } else {
         // TRT + Guo forcing (lbm.py:241-255)
         const float om_m = 1.0f / (0.5f + d.magic / (1.0f / om - 0.5f));
