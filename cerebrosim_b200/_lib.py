@@ -89,6 +89,8 @@ SIGNATURES = {
     "cs_graph_launch": (_I32, [_P, _P]),
     "cs_graph_destroy": (_I32, [_P]),
     "cs_wss_shear": (_I32, [_P, _I64, _P, _P, _P, _I64, _I32, _D, _P, _P]),
+    "cs_probe_gather": (_I32, [_P, _P, _I64, _P, _P, _I32, _P, _P, _P]),
+    "cs_bin_fields": (_I32, [_P, _P, _I64, _P, _P, _I64, _P, _P, _P]),
     "cs_last_error": (_I32, [ctypes.c_char_p, _I32]),
     "cs_version": (ctypes.c_char_p, []),
     "cs_abi_sizeof": (_SZ, [_I32]),

@@ -16,7 +16,7 @@ PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
 OUT = os.path.join(PKG, "libcerebrosim_b200.so")
 OBJ = os.path.join(PKG, "_build")
-SOURCES = ["capi.cu", "sdf.cu", "lattice_build.cu", "links.cu", "compress.cu", "step.cu", "wss.cu"]
+SOURCES = ["capi.cu", "sdf.cu", "lattice_build.cu", "links.cu", "compress.cu", "step.cu", "wss.cu", "gather.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]
 

@@ -113,3 +113,189 @@ class ArterySolver(Solver):
         d.q_part, d.fb_list, d.n_fb = self._q_part.data_ptr(), self._fb_list.data_ptr(), self._n_fb
         d.q_last, d.r_out = self._qlast.data_ptr(), self._r.data_ptr()
         d.pref, d.alpha = self.pref, self.alpha
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# heartbeat loop: probes, coarse-map frames, result files, lumped circuit
+# ---------------------------------------------------------------------------------------------------------------
+
+def _segments(idx, seg, n_seg, n_cells, inv=None):
+    """Cell lists grouped by segment (stable), as device-ready (cells, start) arrays; lattice ids mapped through inv
+    (the solver's internal numbering) when given."""
+    idx = np.asarray(idx, np.int64).reshape(-1)
+    seg = np.asarray(seg, np.int64).reshape(-1)
+    if len(idx) != len(seg):
+        raise ValueError("cell and segment lists differ in length")
+    if len(idx) and (idx.min() < 0 or idx.max() >= n_cells or seg.min() < 0 or seg.max() >= n_seg):
+        raise ValueError("cell index or segment out of range")
+    if inv is not None and len(idx):
+        idx = inv[idx]
+    order = np.argsort(seg, kind="stable")
+    start = np.concatenate([[0], np.cumsum(np.bincount(seg, minlength=n_seg))]).astype(np.int32)
+    return idx[order].astype(np.int32), start
+
+
+class Probes:
+    """Pressure probes (simulate.k_gather, simulate.py:85-90): cells idx[j] (lattice ids) belonging to probe
+    slot[j]. `sample()` -> (mean pressure per probe in lattice units, NaN for a probe without cells; largest speed
+    over all probe cells), reduced on the device in FP64."""
+
+    def __init__(self, s, idx, slot, n_probes):
+        self.s = s
+        self.n = int(n_probes)
+        inv = s.inv.cpu().numpy() if getattr(s, "inv", None) is not None else None
+        cells, start = _segments(idx, slot, self.n, s.N, inv)
+        self.count = np.diff(start)
+        with torch.cuda.device(s.dev):
+            self.cells = torch.as_tensor(cells if len(cells) else np.zeros(1, np.int32)).to(s.dev)
+            self.start = torch.as_tensor(start).to(s.dev)
+            self.psum = torch.zeros(max(1, self.n), dtype=torch.float64, device=s.dev)
+            self.umax = torch.zeros(max(1, self.n), dtype=torch.float32, device=s.dev)
+
+    def sample(self):
+        s = self.s
+        with torch.cuda.device(s.dev), torch.cuda.stream(s.stream):
+            check(_lib.load().cs_probe_gather(ctypes_void(s.rho.data_ptr()), ctypes_void(s.vel[s.cur].data_ptr()),
+                                              s.N, ctypes_void(self.cells.data_ptr()),
+                                              ctypes_void(self.start.data_ptr()), self.n,
+                                              ctypes_void(self.psum.data_ptr()), ctypes_void(self.umax.data_ptr()),
+                                              ctypes_void(s.stream.cuda_stream)))
+        s.stream.synchronize()
+        psum = self.psum.cpu().numpy()[:self.n]
+        p = np.where(self.count > 0, psum / np.maximum(self.count, 1), np.nan)
+        return p, float(self.umax.cpu().numpy()[:self.n].max()) if self.n else 0.0
+
+
+def coarse_bins(lat, dx_mm, target_mm=0.1):
+    """simulate.coarse_map (simulate.py:236-242): cells -> bins of `target_mm` (identity at that spacing, 2x2x2
+    averages at half of it) -> (bin coordinates int16, bin of each cell, cells per bin, factor)."""
+    f = max(1, int(round(target_mm / dx_mm)))
+    key = np.asarray(lat["coords"]) // f
+    uk, inv = np.unique(key, axis=0, return_inverse=True)
+    inv = inv.ravel()
+    return uk.astype(np.int16), inv, np.bincount(inv), f
+
+
+class CoarseMap:
+    """Frames of the stored fields on the coarse bins, averaged on the device: `frame()` -> (p (bins,), u (bins, 3))
+    in lattice units."""
+
+    def __init__(self, s, lat, dx_mm, target_mm=0.1):
+        self.s = s
+        self.uk, self.inv, self.cnt, self.f = coarse_bins(lat, dx_mm, target_mm)
+        self.n_bins = len(self.uk)
+        inv_int = s.inv.cpu().numpy() if getattr(s, "inv", None) is not None else None
+        cells, start = _segments(np.arange(s.N), self.inv, self.n_bins, s.N, inv_int)
+        with torch.cuda.device(s.dev):
+            self.cells = torch.as_tensor(cells).to(s.dev)
+            self.start = torch.as_tensor(start).to(s.dev)
+            self.p = torch.empty(self.n_bins, dtype=torch.float32, device=s.dev)
+            self.u = torch.empty((self.n_bins, 3), dtype=torch.float32, device=s.dev)
+
+    def frame(self):
+        s = self.s
+        with torch.cuda.device(s.dev), torch.cuda.stream(s.stream):
+            check(_lib.load().cs_bin_fields(ctypes_void(s.rho.data_ptr()), ctypes_void(s.vel[s.cur].data_ptr()), s.N,
+                                            ctypes_void(self.cells.data_ptr()), ctypes_void(self.start.data_ptr()),
+                                            self.n_bins, ctypes_void(self.p.data_ptr()), ctypes_void(self.u.data_ptr()),
+                                            ctypes_void(s.stream.cuda_stream)))
+        s.stream.synchronize()
+        return self.p.cpu().numpy(), self.u.cpu().numpy()
+
+
+def run_beats(s, steps_per_beat, beats, every, probes=None, cmap=None, frames=40, on_beat=None):
+    """The measurement loop of simulate.run (simulate.py:300-360) on the device: `every` steps at a time (CUDA
+    graphs), then a sample — time step, flows Qlast and open-end pressures p_out (an ArterySolver), probe pressures
+    and the largest probe speed; `frames` snapshots of the coarse fields evenly over the last beat; `on_beat(s, beat,
+    series)` after each beat (where the reference calibrates its inlet). Lattice units throughout."""
+    if steps_per_beat % every:
+        raise ValueError(f"{steps_per_beat} steps per beat is not a multiple of {every}")
+    frame_every = steps_per_beat // max(1, frames)
+    if frames and frame_every % every:
+        raise ValueError(f"{frame_every} steps per frame is not a multiple of {every}")
+    series = {"step": [], "Q": [], "p_open": [], "p_probe": [], "umax": []}
+    out = {"t_step": [], "p": [], "u": []}
+    total = beats * steps_per_beat
+    coupled = hasattr(s, "Qlast")
+    while s.steps < total:
+        s.run(every, chunk=every)
+        series["step"].append(s.steps)
+        if coupled:
+            series["Q"].append(s.Qlast.numpy().copy())
+            series["p_open"].append(s.p_out.cpu().numpy()[:s.n_open].astype(float))
+        if probes is not None:
+            p, um = probes.sample()
+            series["p_probe"].append(p)
+            series["umax"].append(um)
+        if s.steps % steps_per_beat == 0:
+            if not s.ok():
+                raise RuntimeError(f"solver diverged at step {s.steps}")
+            if on_beat is not None:
+                on_beat(s, s.steps // steps_per_beat, series)
+        last = s.steps - (beats - 1) * steps_per_beat
+        if cmap is not None and frames and last > 0 and last % frame_every == 0:
+            p, u = cmap.frame()
+            out["t_step"].append(last)
+            out["p"].append(p)
+            out["u"].append(u)
+    return {k: np.array(v) for k, v in series.items()}, {k: np.array(v) for k, v in out.items()}
+
+
+def fourier(y, nh=10):
+    """simulate.fourier (simulate.py:123-130): samples over one period -> [a0, a1, b1, a2, b2, ...] of
+    a0 + sum a_k cos(2 pi k t) + b_k sin(2 pi k t)."""
+    F = np.fft.rfft(np.asarray(y, float)) / len(y)
+    c = [F[0].real]
+    for k in range(1, nh + 1):
+        c += [2 * F[k].real, -2 * F[k].imag]
+    return np.array(c)
+
+
+def from_fourier(c, t):
+    """simulate.from_fourier (simulate.py:133-137): the series at times t (in periods)."""
+    y = np.full_like(np.asarray(t, float), c[0], dtype=float)
+    for k in range(1, (len(c) - 1) // 2 + 1):
+        y += c[2 * k - 1] * np.cos(2 * np.pi * k * t) + c[2 * k] * np.sin(2 * np.pi * k * t)
+    return y
+
+
+MMHG = 133.322
+
+
+def circuit(R_seg, shape, q_in_ml_min, q_target_ml_min, p_out_mmhg, nh=10):
+    """simulate.circuit (simulate.py:138-148), SI: the outlets' resistances that split the mean inflow q_in as
+    (q_target, rest) at the mean outlet pressure p_out, and the Fourier coefficients (Pa, absolute) of the inlet
+    pressure that draws the inflow waveform q_in * shape (one period of samples, mean 1) through the segment
+    resistance R_seg plus the outlets in parallel."""
+    q_in = q_in_ml_min * 1e-6 / 60
+    q_t = q_target_ml_min * 1e-6 / 60
+    p_out = p_out_mmhg * MMHG
+    R_t, R_o = p_out / q_t, p_out / (q_in - q_t)
+    R_eq = p_out / q_in
+    coef = fourier((R_eq + R_seg) * q_in * np.asarray(shape, float), nh)
+    return {"R_out": [0.0, R_t, R_o], "R_seg": float(R_seg), "P_in_coef": coef.tolist(), "R_eq": R_eq}
+
+
+def recalibrate(cal, p_in_mean_pa, q_in_mean_ml_min, shape, q_in_ml_min, q_target_ml_min, p_out_mmhg):
+    """The calibrate branch of simulate.run (simulate.py:330-337): the segment resistance implied by a beat's mean
+    inlet pressure and inflow, and the circuit rebuilt with it."""
+    R_tot = p_in_mean_pa / (q_in_mean_ml_min * 1e-6 / 60)
+    return circuit(max(R_tot - cal["R_eq"], 0.0), shape, q_in_ml_min, q_target_ml_min, p_out_mmhg)
+
+
+def save(d, meta, series, frames, cmap=None, lat=None, wall_mm=None, dx_mm=None):
+    """The result files of simulate.save (simulate.py:361-380): series.npz (one array per series), meta.json, and,
+    with frames ({"t", "p_mmhg", "u_m_s"}: one row per frame of the coarse bins, in the caller's units), fields.npz
+    (coarse bin coordinates, origin, dx_mm, wall distance per bin, frame times, p and u as float16)."""
+    import json
+    import os
+    os.makedirs(d, exist_ok=True)
+    np.savez_compressed(os.path.join(d, "series.npz"), **{k: np.asarray(v) for k, v in series.items()})
+    json.dump(meta, open(os.path.join(d, "meta.json"), "w"), indent=1, default=float)
+    if frames is not None and len(frames.get("p_mmhg", [])) and cmap is not None:
+        wall = (np.bincount(cmap.inv, weights=np.asarray(wall_mm, float), minlength=cmap.n_bins) / cmap.cnt
+                if wall_mm is not None else np.zeros(cmap.n_bins))
+        np.savez_compressed(os.path.join(d, "fields.npz"), coords=cmap.uk, origin=np.asarray(lat["origin"]),
+                            dx_mm=0.1 if cmap.f > 1 else (dx_mm if dx_mm is not None else lat["dx"]),
+                            wall_mm=wall.astype(np.float32), t=np.asarray(frames["t"]),
+                            p_mmhg=np.asarray(frames["p_mmhg"], np.float16), u_m_s=np.asarray(frames["u_m_s"], np.float16))

@@ -263,6 +263,21 @@ int cs_wss_shear(const float* U, int64_t n_cells, const int32_t* idx, const floa
                  int64_t n_vert, int32_t K, double scale, float* tau, void* stream);
 
 /* ---------------------------------------------------------------------------------------------------------------
+ * Heartbeat-loop measurements — replace simulate.k_gather (simulate.py:85-90) and the coarse-map averaging of the
+ * stored frames (simulate.py:236-242, 346-353). rho (n) and vel (SoA, 3 * n) are a solver's state buffers; `cells`
+ * lists cell indices (each < n, checked by the caller) grouped by segment, `start` (segments + 1) delimits them.
+ * Sums are FP64 in a fixed order.
+ * ------------------------------------------------------------------------------------------------------------- */
+
+/* Per probe k: psum[k] = sum of rho / 3 over its cells, umax[k] = the largest |u| among them. */
+int cs_probe_gather(const float* rho, const float* vel, int64_t n, const int32_t* cells, const int32_t* start,
+                    int32_t n_probes, double* psum, float* umax, void* stream);
+
+/* Per coarse bin b: p_out[b] = mean of rho / 3 over its cells, u_out[3 b + c] = mean of u_c (0 for an empty bin). */
+int cs_bin_fields(const float* rho, const float* vel, int64_t n, const int32_t* cells, const int32_t* start,
+                  int64_t n_bins, float* p_out, float* u_out, void* stream);
+
+/* ---------------------------------------------------------------------------------------------------------------
  * Misc
  * ------------------------------------------------------------------------------------------------------------- */
 
