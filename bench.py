@@ -42,7 +42,7 @@ DRIVE = ([0.02, 0.0, 0.01], 4000)       # u0 (1 + 0.5 sin(2 pi t / T)): a0 = 0.0
 BPLU = {"f32": 356, "f16": 248, "bf16": 248}   # algorithmic bytes per lattice update
 METRIC = "D3Q27 MLUPS + HBM GB/s on 1 B200, plain vs batched/FP16; p50/p99 beat latency"
 FLUSH_BYTES = 256 << 20
-TUNED = {"block": 256, "order": "c"}     # launch shape of the batched / served forms (set by the sweep's autotuning)
+TUNED = {"block": 128, "order": "c"}     # launch shape of the batched / served forms (set by the sweep's autotuning)
 
 
 def nu_lu():

@@ -29,7 +29,7 @@ class BatchSolver:
     persistent: size the grids to the GPU (SMs x resident blocks) and loop over work items, instead of one block
     per work item."""
 
-    def __init__(self, solvers=(), block=256, persistent=True, device=None):
+    def __init__(self, solvers=(), block=128, persistent=True, device=None):
         self.members = []
         self.block = int(block)
         self.persistent = bool(persistent)

@@ -63,6 +63,10 @@ template <> struct Pop<CS_STORE_F16> {
     static __device__ __forceinline__ void st(void* b, uint32_t idx, float w, float v) {
         static_cast<__half*>(b)[idx] = __float2half_rn(v * (1024.0f / w));
     }
+    // a value already in the stored scale, (f - w) 1024 / w
+    static __device__ __forceinline__ void st_scaled(void* b, uint32_t idx, float g) {
+        static_cast<__half*>(b)[idx] = __float2half_rn(g);
+    }
 };
 
 template <> struct Pop<CS_STORE_BF16> {
@@ -71,6 +75,9 @@ template <> struct Pop<CS_STORE_BF16> {
     }
     static __device__ __forceinline__ void st(void* b, uint32_t idx, float w, float v) {
         static_cast<__nv_bfloat16*>(b)[idx] = __float2bfloat16_rn(v * (1024.0f / w));
+    }
+    static __device__ __forceinline__ void st_scaled(void* b, uint32_t idx, float g) {
+        static_cast<__nv_bfloat16*>(b)[idx] = __float2bfloat16_rn(g);
     }
 };
 
@@ -246,14 +253,21 @@ __device__ __forceinline__ void moments27(const float (&f)[Q], Moments& m) {
     m.jz = dp[2] + dp[5] - dp[6] + dp[7] - dp[8] + (dpr + dpt);
 }
 
-// One pair's outputs w (A + e +- o) (the weight is the pair's).
+// One pair's outputs: FP32 stores w (A + e +- o); the 16-bit formats store (f - w) 1024 / w = 1024 (A + e +- o),
+// for which A, e and o arrive already multiplied by 1024 (no per-link weight or scale left to apply).
 template <int ST, int I>
 __device__ __forceinline__ void store_pair(void* fout, uint32_t NP, int32_t n, float A, float e, float o) {
     constexpr int O = Lat::opp(I);
-    constexpr float w = wgt(I);
-    const float wb = w * (A + e);
-    Pop<ST>::st(fout, uint32_t(I) * NP + uint32_t(n), w, fmaf(w, o, wb));
-    Pop<ST>::st(fout, uint32_t(O) * NP + uint32_t(n), w, fmaf(-w, o, wb));
+    if constexpr (ST == CS_STORE_F32) {
+        constexpr float w = wgt(I);
+        const float wb = w * (A + e);
+        Pop<ST>::st(fout, uint32_t(I) * NP + uint32_t(n), w, fmaf(w, o, wb));
+        Pop<ST>::st(fout, uint32_t(O) * NP + uint32_t(n), w, fmaf(-w, o, wb));
+    } else {
+        const float b = A + e;
+        Pop<ST>::st_scaled(fout, uint32_t(I) * NP + uint32_t(n), b + o);
+        Pop<ST>::st_scaled(fout, uint32_t(O) * NP + uint32_t(n), b - o);
+    }
 }
 
 // Regularised collision output without a body force (lbm.py:129-137, 230-240): f_I = w_I (A + e_I + o_I) and
@@ -264,7 +278,20 @@ template <int ST, bool GAL>
 __device__ __forceinline__ void store_regularised(void* fout, uint32_t NP, int32_t n, float A, float ux, float uy,
                                                   float uz, float mxx, float myy, float mzz, float mxy2,
                                                   float mxz2, float myz2) {
-    Pop<ST>::st(fout, uint32_t(n), wgt(0), wgt(0) * A);
+    // SC: the stored scale (1024 for the 16-bit formats, applied to A, M and the constants; exact in binary)
+    constexpr float SC = ST == CS_STORE_F32 ? 1.0f : 1024.0f;
+    if constexpr (ST == CS_STORE_F32) {
+        Pop<ST>::st(fout, uint32_t(n), wgt(0), wgt(0) * A);
+    } else {
+        A *= SC;
+        mxx *= SC;
+        myy *= SC;
+        mzz *= SC;
+        mxy2 *= SC;
+        mxz2 *= SC;
+        myz2 *= SC;
+        Pop<ST>::st_scaled(fout, uint32_t(n), A);
+    }
     // third-order terms from the velocity monomials: axis links -4.5 (sum of two), edges 9 (..) - 4.5 (..),
     // corners 9 (+-A1 +-A2 +-A3) +- 27 xyz
     float h1 = 0.f, h3 = 0.f, h5 = 0.f, h7 = 0.f, h9 = 0.f, h11 = 0.f, h13 = 0.f, h15 = 0.f, h17 = 0.f;
@@ -274,16 +301,16 @@ __device__ __forceinline__ void store_regularised(void* fout, uint32_t NP, int32
         const float xxy = x2 * uy, xxz = x2 * uz, xyy = ux * y2, yyz = y2 * uz, xzz = ux * z2, yzz = uy * z2;
         const float xyz = ux * uy * uz;
         const float a1 = xxy + yzz, a2 = xxz + yyz, a3 = xyy + xzz;
-        h1 = -4.5f * a3;
-        h3 = -4.5f * a1;
-        h5 = -4.5f * a2;
-        h7 = 9.0f * (xyy + xxy) - 4.5f * (xzz + yzz);
-        h9 = 9.0f * (xyy - xxy) - 4.5f * (xzz - yzz);
-        h11 = 9.0f * (xzz + xxz) - 4.5f * (xyy + yyz);
-        h13 = 9.0f * (xzz - xxz) - 4.5f * (xyy - yyz);
-        h15 = 9.0f * (yzz + yyz) - 4.5f * (xxy + xxz);
-        h17 = 9.0f * (yzz - yyz) - 4.5f * (xxy - xxz);
-        const float b1 = 9.0f * a1, b2 = 9.0f * a2, b3 = 9.0f * a3, bx = 27.0f * xyz;
+        h1 = (-4.5f * SC) * a3;
+        h3 = (-4.5f * SC) * a1;
+        h5 = (-4.5f * SC) * a2;
+        h7 = (9.0f * SC) * (xyy + xxy) - (4.5f * SC) * (xzz + yzz);
+        h9 = (9.0f * SC) * (xyy - xxy) - (4.5f * SC) * (xzz - yzz);
+        h11 = (9.0f * SC) * (xzz + xxz) - (4.5f * SC) * (xyy + yyz);
+        h13 = (9.0f * SC) * (xzz - xxz) - (4.5f * SC) * (xyy - yyz);
+        h15 = (9.0f * SC) * (yzz + yyz) - (4.5f * SC) * (xxy + xxz);
+        h17 = (9.0f * SC) * (yzz - yyz) - (4.5f * SC) * (xxy - xxz);
+        const float b1 = (9.0f * SC) * a1, b2 = (9.0f * SC) * a2, b3 = (9.0f * SC) * a3, bx = (27.0f * SC) * xyz;
         const float p_ = b1 + b3, q_ = b2 + bx, m_ = b3 - b1, n_ = b2 - bx;
         h19 = p_ + q_;
         h21 = p_ - q_;
@@ -291,32 +318,30 @@ __device__ __forceinline__ void store_regularised(void* fout, uint32_t NP, int32
         h25 = n_ - m_;
     }
     // axis
-    store_pair<ST, 1>(fout, NP, n, A, mxx, 3.0f * ux + h1);
-    store_pair<ST, 3>(fout, NP, n, A, myy, 3.0f * uy + h3);
-    store_pair<ST, 5>(fout, NP, n, A, mzz, 3.0f * uz + h5);
+    store_pair<ST, 1>(fout, NP, n, A, mxx, (3.0f * SC) * ux + h1);
+    store_pair<ST, 3>(fout, NP, n, A, myy, (3.0f * SC) * uy + h3);
+    store_pair<ST, 5>(fout, NP, n, A, mzz, (3.0f * SC) * uz + h5);
     // edges, plane by plane
     const float sxy = mxx + myy, sxz = mxx + mzz, syz = myy + mzz;
     const float u7 = ux + uy, u9 = ux - uy;
-    store_pair<ST, 7>(fout, NP, n, A, sxy + mxy2, 3.0f * u7 + h7);
-    store_pair<ST, 9>(fout, NP, n, A, sxy - mxy2, 3.0f * u9 + h9);
-    store_pair<ST, 11>(fout, NP, n, A, sxz + mxz2, 3.0f * (ux + uz) + h11);
-    store_pair<ST, 13>(fout, NP, n, A, sxz - mxz2, 3.0f * (ux - uz) + h13);
-    store_pair<ST, 15>(fout, NP, n, A, syz + myz2, 3.0f * (uy + uz) + h15);
-    store_pair<ST, 17>(fout, NP, n, A, syz - myz2, 3.0f * (uy - uz) + h17);
+    store_pair<ST, 7>(fout, NP, n, A, sxy + mxy2, (3.0f * SC) * u7 + h7);
+    store_pair<ST, 9>(fout, NP, n, A, sxy - mxy2, (3.0f * SC) * u9 + h9);
+    store_pair<ST, 11>(fout, NP, n, A, sxz + mxz2, (3.0f * SC) * (ux + uz) + h11);
+    store_pair<ST, 13>(fout, NP, n, A, sxz - mxz2, (3.0f * SC) * (ux - uz) + h13);
+    store_pair<ST, 15>(fout, NP, n, A, syz + myz2, (3.0f * SC) * (uy + uz) + h15);
+    store_pair<ST, 17>(fout, NP, n, A, syz - myz2, (3.0f * SC) * (uy - uz) + h17);
     // corners
     const float tr = sxy + mzz, ca = tr + mxy2, cb = tr - mxy2, cg = mxz2 + myz2, cd = mxz2 - myz2;
-    store_pair<ST, 19>(fout, NP, n, A, ca + cg, 3.0f * (u7 + uz) + h19);
-    store_pair<ST, 21>(fout, NP, n, A, ca - cg, 3.0f * (u7 - uz) + h21);
-    store_pair<ST, 23>(fout, NP, n, A, cb + cd, 3.0f * (u9 + uz) + h23);
-    store_pair<ST, 25>(fout, NP, n, A, cb - cd, 3.0f * (uz - u9) + h25);
+    store_pair<ST, 19>(fout, NP, n, A, ca + cg, (3.0f * SC) * (u7 + uz) + h19);
+    store_pair<ST, 21>(fout, NP, n, A, ca - cg, (3.0f * SC) * (u7 - uz) + h21);
+    store_pair<ST, 23>(fout, NP, n, A, cb + cd, (3.0f * SC) * (u9 + uz) + h23);
+    store_pair<ST, 25>(fout, NP, n, A, cb - cd, (3.0f * SC) * (uz - u9) + h25);
 }
 
 // ---- 1. boundary-link kernel and clock ----------------------------------------------------------------------------
-// Block (bx, by) of a lattice's boundary-link grid: by = direction, bx = chunk of its ghost slots. Called by every
-// thread of the block (it synchronises the block once).
+// Block (bx, by) of a lattice's boundary-link grid: by = direction, bx = chunk of its ghost slots.
 template <int ST>
 __device__ __forceinline__ void boundary_body(const cs_step_desc& d, const int a, const int bx, const int by) {
-    __shared__ float s_drive;
     // the ghost table is static: read it before waiting for the previous kernel of the stream
     const int i = by;
     const int64_t g = int64_t(bx) * B_THREADS + threadIdx.x;
@@ -358,15 +383,13 @@ __device__ __forceinline__ void boundary_body(const cs_step_desc& d, const int a
             pk = __ldg(d.p_out + (CS_OUTLET0 - info));
         }
     }
-    if (threadIdx.x == 0) {
+    // the clock: the first thread of the grid publishes this step's drive and advances the tick; an inlet link
+    // evaluates the drive itself (no block waits for one thread's evaluation)
+    if (threadIdx.x == 0 && bx == 0 && by == 0) {
         const int t = d.tick[a];
-        s_drive = drive_value(d, t);
-        if (bx == 0 && by == 0) {
-            *d.drive = s_drive;
-            d.tick[1 - a] = t + 1;
-        }
+        *d.drive = drive_value(d, t);
+        d.tick[1 - a] = t + 1;
     }
-    __syncthreads();
     launch_dependents();                                    // the bulk kernel may start its static loads
     if (!live_node) return;                                 // padding slot of a direction with fewer links
     const float cx = float(k_cx[i]), cy = float(k_cy[i]), cz = float(k_cz[i]);
@@ -384,7 +407,7 @@ __device__ __forceinline__ void boundary_body(const cs_step_desc& d, const int a
         }
     } else if (is_inlet) {
         // lbm.py:174-177: bounce-back with the prescribed velocity
-        const float dv = s_drive;
+        const float dv = drive_value(d, d.tick[a]);
         const float cu = cx * (e0 * dv) + cy * (e1 * dv) + cz * (e2 * dv);
         v = fo + 6.0f * w * cu;
     } else {
@@ -961,7 +984,6 @@ __global__ void __launch_bounds__(B_THREADS) k_boundary_batch(const __grid_const
         const cs_step_desc& d = g.d[cur.inst];
         const int nbx = int(max(int64_t(1), ceil_div(d.gmax, B_THREADS)));
         boundary_body<ST>(d, a ^ g.parity[cur.inst], local % nbx, local / nbx);
-        __syncthreads();                        // boundary_body keeps the drive in shared memory
     }
     // the previous bulk kernel has finished (boundary_body waited for it) and the next one takes no item before
     // this kernel ends: reset its work counter

@@ -80,7 +80,7 @@ class Server:
     launch shape and node order of every request's solver (autotune.tune picks them)."""
 
     def __init__(self, budget_bytes=150e9, storage="bf16", steps_per_beat=8000, chunk=1000, graph_chunk=200,
-                 max_active=64, block=256, ahead=2, keep_fields=True, device=None, builder=default_builder,
+                 max_active=64, block=128, ahead=2, keep_fields=True, device=None, builder=default_builder,
                  order="c"):
         if steps_per_beat % chunk or chunk % 2 or graph_chunk % 2:
             raise ValueError("chunk must divide steps_per_beat; chunk and graph_chunk must be even")
@@ -212,7 +212,7 @@ def summary(reqs, steps_per_beat):
             "all_ok": bool(all(r.ok for r in reqs))}
 
 
-def one_by_one(specs, storage="f32", steps_per_beat=8000, graph_chunk=200, block=256, device=None,
+def one_by_one(specs, storage="f32", steps_per_beat=8000, graph_chunk=200, block=None, device=None,
                builder=default_builder, order="c"):
     """The same requests run one after another, each on its own dedicated solver (plain form): total seconds,
     lattice updates and MLUPS, builds included as in the served stream."""

@@ -200,7 +200,7 @@ def configure(s, spec, lat, period=8000, ramp=1000, sponge=(8, 0.6)):
     return s
 
 
-def make_solver(spec, lat, tau=0.52, period=8000, ramp=1000, storage="f32", block=256, sponge=(8, 0.6),
+def make_solver(spec, lat, tau=0.52, period=8000, ramp=1000, storage="f32", block=None, sponge=(8, 0.6),
                 device=None, order="c"):
     """Solver for a spec on its lattice (tau, regularised collision), configured by `configure`."""
     s = lbm.Solver(lat, (tau - 0.5) / 3.0, model="regularised", storage=storage, block=block, device=device,
@@ -208,7 +208,7 @@ def make_solver(spec, lat, tau=0.52, period=8000, ramp=1000, storage="f32", bloc
     return configure(s, spec, lat, period, ramp, sponge)
 
 
-def build_spec(spec, storage="f32", block=256, device=None, **kw):
+def build_spec(spec, storage="f32", block=None, device=None, **kw):
     """Vessel, lattice and solver of a spec -> (solver, geometry, lattice, dx)."""
     g, lat, dx = spec_lattice(spec, device=device)
     return make_solver(spec, lat, storage=storage, block=block, device=device, **kw), g, lat, dx
