@@ -190,6 +190,7 @@ def bench_sweep(args, dev, peak):
     # block size and node order: tuned on the largest vessel, for its storage format, then used by every member
     big = max(range(len(specs)), key=lambda k: lats[k]["nbr"].shape[1])
     best, table = autotune.tune(lats[big], (0.52 - 0.5) / 3.0, storage=args.sweep_storage, steps=200, warmup=50,
+                                blocks=(128, 256),
                                 configure=lambda s: W.configure(s, specs[big], lats[big]), device=dev,
                                 model="regularised")
     TUNED.update(block=best["block"], order=best["order"])
@@ -297,7 +298,12 @@ def main():
     c = cases.case(WORKLOAD)
     lat = plug_inlet(lbm.build_lattice(**cases.lattice_args(c), device=dev))
     N = lat["nbr"].shape[1]
-    s = lbm.Solver(lat, nu_lu(), model="regularised", device=dev, storage=args.storage)
+    # launch shape and node order chosen by the autotuner (short timed runs of each candidate on this lattice)
+    from cerebrosim_b200 import autotune
+    tuned, tune_table = autotune.tune(lat, nu_lu(), configure=configure, storage=args.storage, blocks=(128, 256),
+                                      orders=("c", "split"), steps=400, warmup=100, device=dev, model="regularised")
+    shape = {"block": tuned["block"], "order": tuned["order"]}
+    s = lbm.Solver(lat, nu_lu(), model="regularised", device=dev, storage=args.storage, **shape)
     configure(s)
     lib = _lib.load()
     stream = s.stream
@@ -366,7 +372,7 @@ def main():
     h2d = sum(host[k].numel() * host[k].element_size() for k in ("nbr", "q", "uin"))
     launches_per_step = 2                     # boundary-link kernel + bulk kernel
     del s
-    warm = lbm.Solver(host, nu_lu(), model="regularised", device=dev, storage=args.storage)   # untimed warm-up
+    warm = lbm.Solver(host, nu_lu(), model="regularised", device=dev, storage=args.storage, **shape)   # untimed
     configure(warm)
     warm.run(4)
     warm.fields()
@@ -375,7 +381,7 @@ def main():
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    s2 = lbm.Solver(host, nu_lu(), model="regularised", device=dev, storage=args.storage)
+    s2 = lbm.Solver(host, nu_lu(), model="regularised", device=dev, storage=args.storage, **shape)
     configure(s2)
     s2.run(args.steps)
     p_h, u_h = s2.fields()
@@ -396,6 +402,8 @@ def main():
                                        "inlet u0 (1 + 0.5 sin(2 pi t / 4000)), pressure outlet, regularised + "
                                        "Galilean + Bouzidi",
                            "storage": args.storage, "nodes": N, "parallelism": f"replicas x{world}",
+                           "block": shape["block"], "order": shape["order"],
+                           "autotune": tune_table,
                            "l2": "flushed between timed steps: 256 MB write then 256 MB read, outside the "
                                  "timed region (cold inputs, no dirty lines left in L2)"},
                 "hbm_gbs": achieved,

@@ -440,18 +440,26 @@ class Solver:
             pass
 
 
-ORDERS = ("c", "axis", "morton")
+ORDERS = ("c", "axis", "morton", "split", "axis-split")
 
 
 def node_order(lat, order="c"):
     """Internal numbering of a lattice's nodes (internal node k = lattice node perm[k]); None for the lattice's own
     C order. "axis": C order with the axis of largest extent varying fastest (long runs along a vessel); "morton":
-    Z-order curve of the grid coordinates."""
+    Z-order curve of the grid coordinates; "split" / "axis-split": C / axis order with the nodes that have a
+    boundary link moved after all others (so the boundary-link kernel reads consecutive nodes and the bulk
+    kernel's warps are all plain or all boundary)."""
     if order not in ORDERS:
         raise ValueError(f"order {order!r}: one of {ORDERS}")
     if order == "c" or lat["nbr"].shape[1] == 0:
         return None
     c = np.asarray(lat["coords"], np.int64)
+    if order.endswith("split"):
+        base = node_order(lat, "axis") if order == "axis-split" else None
+        base = np.arange(len(c)) if base is None else base
+        bnd = (np.asarray(lat["nbr"]) < 0).any(0)[base]
+        perm = np.concatenate([base[~bnd], base[bnd]])
+        return None if np.array_equal(perm, np.arange(len(perm))) else perm
     if order == "axis":
         ext = c.max(0) - c.min(0)
         fast = int(np.argmax(ext))

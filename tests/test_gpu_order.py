@@ -28,7 +28,7 @@ def test_orders_give_identical_fields(golden, storage):
     configure(ref)
     ref.run(301)
     p0, u0 = ref.fields()
-    for order in ("axis", "morton"):
+    for order in ("axis", "morton", "split", "axis-split"):
         s = lbm.Solver(lat, 0.02, model="regularised", storage=storage, order=order)
         assert order == "axis" or s.perm is not None
         configure(s)
@@ -48,7 +48,7 @@ def test_artery_coupling_in_another_order(golden):
     flux = {"idx": idx, "w": np.tile(np.array([[0, 0, 0.5]], np.float32), (len(idx), 1)),
             "slot": (z[idx] > 10).astype(int)}
     runs = []
-    for order in ("c", "morton"):
+    for order in ("c", "split"):
         s = ArterySolver(lat, 0.01, flux, [0.0, 0.05], 1e-4, 0.01, model="regularised", order=order)
         s.set_outlet_pressure([0.0, -1e-4])
         s.set_sponge(4, 0.55, kinds=("outlet",))

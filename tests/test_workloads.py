@@ -96,3 +96,15 @@ def test_node_orders_are_permutations():
     perm = lbm.node_order({"coords": long_x, "nbr": lat["nbr"]}, "axis")
     c = long_x[perm]
     assert np.all(np.diff(c[:, 0])[(np.diff(c[:, 2]) == 0) & (np.diff(c[:, 1]) == 0)] > 0)
+
+
+def test_split_order_puts_boundary_nodes_last():
+    from cerebrosim_b200 import cases, lbm
+    from oracle import lattice_ref as L
+    lat = L.build_lattice(**cases.lattice_args(cases.case("open_pipe_straight_D20")))
+    bnd = (lat["nbr"] < 0).any(0)
+    perm = lbm.node_order(lat, "split")
+    assert np.array_equal(np.sort(perm), np.arange(len(perm)))
+    k = int((~bnd).sum())
+    assert not bnd[perm[:k]].any() and bnd[perm[k:]].all()
+    assert np.all(np.diff(perm[:k]) > 0) and np.all(np.diff(perm[k:]) > 0)      # C order within each part
