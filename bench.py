@@ -298,10 +298,12 @@ def main():
     c = cases.case(WORKLOAD)
     lat = plug_inlet(lbm.build_lattice(**cases.lattice_args(c), device=dev))
     N = lat["nbr"].shape[1]
-    # launch shape and node order chosen by the autotuner (short timed runs of each candidate on this lattice)
+    # block size chosen by the autotuner (short timed runs of each candidate on this lattice); the reference's node
+    # order (the split order gains ~3 % back to back but nothing with a cold L2, and costs the end-to-end path its
+    # renumbering)
     from cerebrosim_b200 import autotune
     tuned, tune_table = autotune.tune(lat, nu_lu(), configure=configure, storage=args.storage, blocks=(128, 256),
-                                      orders=("c", "split"), steps=400, warmup=100, device=dev, model="regularised")
+                                      orders=("c",), steps=400, warmup=100, device=dev, model="regularised")
     shape = {"block": tuned["block"], "order": tuned["order"]}
     s = lbm.Solver(lat, nu_lu(), model="regularised", device=dev, storage=args.storage, **shape)
     configure(s)
