@@ -77,11 +77,13 @@ class Server:
     budget_bytes: device memory the resident requests may hold (admission control); max_active: largest batch;
     chunk: steps per scheduling round (a divisor of steps_per_beat); graph_chunk: steps per captured graph;
     ahead: chunks kept enqueued; keep_fields: read each result's (p, u) back to the host; block and order: the
-    launch shape and node order of every request's solver (autotune.tune picks them)."""
+    launch shape and node order of every request's solver (autotune.tune picks them); on_beat(request, beat): called
+    when a request completes a beat (not its last), with its solver's state final for that beat — what it changes
+    (a recalibrated drive: simulate.recalibrate) applies from the next beat's first step."""
 
     def __init__(self, budget_bytes=150e9, storage="bf16", steps_per_beat=8000, chunk=1000, graph_chunk=200,
                  max_active=64, block=128, ahead=2, keep_fields=True, device=None, builder=default_builder,
-                 order="c"):
+                 order="c", on_beat=None):
         if steps_per_beat % chunk or chunk % 2 or graph_chunk % 2:
             raise ValueError("chunk must divide steps_per_beat; chunk and graph_chunk must be even")
         self.budget = float(budget_bytes)
@@ -96,6 +98,7 @@ class Server:
         self.device = device
         self.builder = builder
         self.order = order
+        self.on_beat = on_beat
         self.trace = []         # (seconds, active requests, reserved bytes) after each admission
 
     def estimate(self, spec):
@@ -125,6 +128,27 @@ class Server:
                 r.fields = s.fields()
         r.solver = None
 
+    def _complete(self, item, base, start):
+        """A chunk has completed: record beat ends, call on_beat, finish the requests it ended; returns the bytes
+        those requests release."""
+        ev, snap = item
+        ev.synchronize()
+        t = base + start.elapsed_time(ev) / 1e3
+        freed = 0.0
+        for r, steps in snap:
+            if steps % self.steps_per_beat == 0:
+                r.beat_end.append(t)
+                if self.on_beat is not None and steps < r.steps_total:
+                    self.on_beat(r, steps // self.steps_per_beat)
+            if steps >= r.steps_total:
+                self._finish(r, t)
+                freed += r.bytes_reserved
+        return freed
+
+    def _drain(self, inflight, base, start, active):
+        while inflight:
+            self._used -= self._complete(inflight.popleft(), base, start)
+
     def serve(self, specs, realtime=True):
         """Serve the requests (arrival times in seconds from now when realtime, else all queued at once, in
         arrival order) -> list of `Request` in arrival order, with timings and results."""
@@ -137,7 +161,7 @@ class Server:
         queue = collections.deque()
         active = []
         inflight = collections.deque()     # (event, [(request, steps enqueued after this chunk)])
-        used = 0.0
+        self._used = 0.0
         batch = None
         self._side = torch.cuda.Stream(self.device)
         t0 = time.perf_counter()
@@ -150,7 +174,7 @@ class Server:
             while queue and len(active) < self.max_active:
                 r = queue[0]
                 need = self.estimate(r.spec)
-                if used + need > self.budget:
+                if self._used + need > self.budget:
                     if not active and not inflight:
                         raise RuntimeError(f"request {r.id} needs ~{need / 1e9:.1f} GB, over the "
                                            f"{self.budget / 1e9:.1f} GB budget")
@@ -163,10 +187,15 @@ class Server:
                     start = torch.cuda.Event(enable_timing=True)
                     start.record(batch.stream)
                     base = time.perf_counter() - t0
-                used += max(need, r.bytes)
+                self._used += max(need, r.bytes)
                 r.bytes_reserved = max(need, r.bytes)
                 active.append(r)
-                self.trace.append((r.admit, len(active), used))
+                self.trace.append((r.admit, len(active), self._used))
+            if active and self.on_beat is not None and inflight and any(
+                    0 < r.steps_enq < r.steps_total and r.steps_enq % self.steps_per_beat == 0 for r in active):
+                # a member has just been given its beat's last chunk: let it finish, so that on_beat sees the beat's
+                # final state and what it changes applies from the next beat's first step (simulate.py:330-337)
+                self._drain(inflight, base, start, active)
             if active:
                 batch.run(self.chunk, chunk=self.graph_chunk)
                 ev = torch.cuda.Event(enable_timing=True)
@@ -181,15 +210,7 @@ class Server:
                     active.remove(r)
             # completed chunks: beat ends, finished requests (their buffers are final once the event has passed)
             while inflight and (len(inflight) > self.ahead or not active or inflight[0][0].query()):
-                ev, snap = inflight.popleft()
-                ev.synchronize()
-                t = base + start.elapsed_time(ev) / 1e3
-                for r, steps in snap:
-                    if steps % self.steps_per_beat == 0:
-                        r.beat_end.append(t)
-                    if steps >= r.steps_total:
-                        self._finish(r, t)
-                        used -= r.bytes_reserved
+                self._used -= self._complete(inflight.popleft(), base, start)
                 if not active:
                     break
             if not active and not inflight and not queue and pending and realtime:

@@ -77,3 +77,21 @@ def test_request_over_budget_is_refused():
     sv = server("bf16", budget_bytes=1e6)
     with pytest.raises(RuntimeError, match="budget"):
         sv.serve(specs()[:1], realtime=False)
+
+
+def test_on_beat_changes_apply_from_the_next_beat():
+    """A per-beat hook (where the lumped circuit is recalibrated, simulate.py:330-337) rescales each request's drive
+    after its first beat: served in a mix, the result equals the same schedule run on a dedicated solver."""
+    def rescale(r, beat):
+        s = r.solver
+        s.set_drive([1.2 * c for c in s.coef.cpu().numpy()[:1 + 2 * s.nh]], period=s.period, ramp=s.ramp)
+
+    sp = [dict(x, beats=2) for x in specs()[:3]]
+    mix = server("f32", max_active=3, on_beat=rescale).serve(sp, realtime=False)
+    for r in mix:
+        s = serve.default_builder(r.spec, "f32", 128, None, SPB)
+        s.run(SPB, chunk=50)
+        s.set_drive([1.2 * c for c in s.coef.cpu().numpy()[:1 + 2 * s.nh]], period=s.period, ramp=s.ramp)
+        s.run(SPB, chunk=50)
+        p, u = s.fields()
+        assert l2(r.fields[1], u) <= 1e-5, r.id
