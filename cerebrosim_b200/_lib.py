@@ -46,7 +46,8 @@ class StepDesc(ctypes.Structure):
                 ("flux_w", ctypes.c_void_p), ("flux_slot", ctypes.c_void_p), ("flux_block", ctypes.c_void_p),
                 ("q_part", ctypes.c_void_p), ("fb_list", ctypes.c_void_p), ("n_fb", ctypes.c_int32),
                 ("q_last", ctypes.c_void_p), ("p_out64", ctypes.c_void_p),
-                ("r_out", ctypes.c_void_p), ("pref", ctypes.c_double), ("alpha", ctypes.c_double)]
+                ("r_out", ctypes.c_void_p), ("pref", ctypes.c_double), ("alpha", ctypes.c_double),
+                ("gblock", ctypes.c_int32 * 28)]
 
 
 class BatchDesc(ctypes.Structure):

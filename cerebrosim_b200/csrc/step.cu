@@ -341,7 +341,8 @@ __device__ __forceinline__ void store_regularised(void* fout, uint32_t NP, int32
 // ---- 1. boundary-link kernel and clock ----------------------------------------------------------------------------
 // Block (bx, by) of a lattice's boundary-link grid: by = direction, bx = chunk of its ghost slots.
 template <int ST>
-__device__ __forceinline__ void boundary_body(const cs_step_desc& d, const int a, const int bx, const int by) {
+__device__ __forceinline__ void boundary_body(const cs_step_desc& d, const int a, const int bx, const int by,
+                                              const bool clock) {
     // the ghost table is static: read it before waiting for the previous kernel of the stream
     const int i = by;
     const int64_t g = int64_t(bx) * B_THREADS + threadIdx.x;
@@ -385,7 +386,7 @@ __device__ __forceinline__ void boundary_body(const cs_step_desc& d, const int a
     }
     // the clock: the first thread of the grid publishes this step's drive and advances the tick; an inlet link
     // evaluates the drive itself (no block waits for one thread's evaluation)
-    if (threadIdx.x == 0 && bx == 0 && by == 0) {
+    if (threadIdx.x == 0 && clock) {
         const int t = d.tick[a];
         *d.drive = drive_value(d, t);
         d.tick[1 - a] = t + 1;
@@ -419,9 +420,38 @@ __device__ __forceinline__ void boundary_body(const cs_step_desc& d, const int a
     Pop<ST>::st(d.f[a], uint32_t(i) * NP + uint32_t(d.n + g), w, v);
 }
 
+// Direction of block b of the unpadded boundary grid: the largest i with gblock[i] <= b.
+__device__ __forceinline__ int grid_direction(const int32_t* gblock, int b) {
+    int lo = 0, hi = Q - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (gblock[mid] <= b) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Work item `item` of a lattice's boundary-link grid: a 256-slot chunk of one direction (unpadded grid when gblock
+// is set, else ceil(gmax / 256) chunks per direction); item 0 advances the clock.
+template <int ST>
+__device__ __forceinline__ void boundary_item(const cs_step_desc& d, const int a, const int item) {
+    if (d.gblock[Q] > 0) {
+        const int i = grid_direction(d.gblock, item);
+        boundary_body<ST>(d, a, item - d.gblock[i], i, item == 0);
+    } else {
+        const int nbx = int(max(int64_t(1), ceil_div(d.gmax, B_THREADS)));
+        boundary_body<ST>(d, a, item % nbx, item / nbx, item == 0);
+    }
+}
+
+__host__ __device__ __forceinline__ int boundary_items(const cs_step_desc& d) {
+    if (d.gblock[Q] > 0) return d.gblock[Q];
+    const int64_t nbx = d.gmax > 0 ? (d.gmax + B_THREADS - 1) / B_THREADS : 1;
+    return int(Q * nbx);
+}
+
 template <int ST>
 __global__ void __launch_bounds__(B_THREADS) k_boundary(const cs_step_desc d, const int a) {
-    boundary_body<ST>(d, a, blockIdx.x, blockIdx.y);
+    boundary_item<ST>(d, a, blockIdx.x);
 }
 
 // ---- 2. bulk kernel -----------------------------------------------------------------------------------------------
@@ -782,6 +812,13 @@ int validate(const cs_step_desc* d) {
     if (d->n < 0 || d->n >= (int64_t(1) << 30)) return fail(CS_ERR_SIZE, "cs_step: n = %lld", (long long)d->n);
     if (d->gmax < 0 || d->npad != d->n + d->gmax || int64_t(Q) * d->npad >= (int64_t(1) << 31))
         return fail(CS_ERR_SIZE, "cs_step: npad %lld must be n + gmax with 27 * npad < 2^31", (long long)d->npad);
+    if (d->gblock[0] != 0) return fail(CS_ERR_ARG, "cs_step: gblock[0] = %d", d->gblock[0]);
+    for (int i = 0; i < Q; ++i) {
+        const int64_t w = int64_t(d->gblock[i + 1]) - d->gblock[i];
+        if (w < 0 || w * B_THREADS > std::max<int64_t>(d->gmax, 0) + B_THREADS - 1)
+            return fail(CS_ERR_ARG, "cs_step: gblock[%d..%d] = %d..%d for gmax %lld", i, i + 1, d->gblock[i],
+                        d->gblock[i + 1], (long long)d->gmax);
+    }
     if (d->storage < 0 || d->storage > 2) return fail(CS_ERR_ARG, "cs_step: storage %d", d->storage);
     if (d->model != CS_MODEL_TRT && d->model != CS_MODEL_REGULARISED) return fail(CS_ERR_ARG, "cs_step: model %d", d->model);
     if (d->block != 0 && (d->block < 32 || d->block > MAX_BLOCK || d->block % 32))
@@ -821,7 +858,7 @@ int launch_pdl(StepFn fn, dim3 grid, dim3 block, cudaStream_t st, const cs_step_
 int launch_steps(const cs_step_desc* d, int a, int steps, cudaStream_t st) {
     const int block = d->block ? d->block : MAX_BLOCK;
     const unsigned grid = unsigned(d->n > 0 ? ceil_div(d->n, block) : 0);
-    const dim3 bgrid(unsigned(std::max<int64_t>(1, ceil_div(d->gmax, B_THREADS))), Q);
+    const dim3 bgrid(unsigned(boundary_items(*d)));
     StepFn bulk = pick_bulk(*d);
     StepFn bound = pick_boundary(*d);
     for (int s = 0; s < steps; ++s) {
@@ -981,9 +1018,7 @@ __global__ void __launch_bounds__(B_THREADS) k_boundary_batch(const __grid_const
     InstanceCursor cur(g.bnd_prefix, g.n_inst);
     for (int item = r.lo; item < r.hi; ++item) {
         const int local = cur.next(item);
-        const cs_step_desc& d = g.d[cur.inst];
-        const int nbx = int(max(int64_t(1), ceil_div(d.gmax, B_THREADS)));
-        boundary_body<ST>(d, a ^ g.parity[cur.inst], local % nbx, local / nbx);
+        boundary_item<ST>(g.d[cur.inst], a ^ g.parity[cur.inst], local);
     }
     // the previous bulk kernel has finished (boundary_body waited for it) and the next one takes no item before
     // this kernel ends: reset its work counter
@@ -1060,7 +1095,7 @@ int validate_batch(const cs_batch_desc* b) {
             return fail(CS_ERR_ARG, "cs_batch_step: instance %d has open ends but the batch has any_open = 0", i);
         if (b->parity[i] != 0 && b->parity[i] != 1)
             return fail(CS_ERR_ARG, "cs_batch_step: parity[%d] = %d", i, b->parity[i]);
-        items += ceil_div(d.n, int64_t(b->block)) + int64_t(Q) * std::max(int64_t(1), ceil_div(d.gmax, int64_t(B_THREADS)));
+        items += ceil_div(d.n, int64_t(b->block)) + boundary_items(d);
     }
     if (items > INT32_MAX - int64_t(MAX_BLOCK) * 2048)
         return fail(CS_ERR_SIZE, "cs_batch_step: %lld work items", (long long)items);
@@ -1083,7 +1118,7 @@ std::vector<BatchGroup> make_groups(const cs_batch_desc* b) {
             g.bulk_prefix[k] = int32_t(bulk);
             g.bnd_prefix[k] = int32_t(bnd);
             bulk += ceil_div(d.n, int64_t(b->block));
-            bnd += Q * std::max(int64_t(1), ceil_div(d.gmax, int64_t(B_THREADS)));
+            bnd += boundary_items(d);
         }
         g.bulk_prefix[g.n_inst] = int32_t(bulk);
         g.bnd_prefix[g.n_inst] = int32_t(bnd);

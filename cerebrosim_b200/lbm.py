@@ -325,6 +325,11 @@ class Solver:
     def _desc(self):
         d = _lib.StepDesc()
         d.n, d.npad, d.gmax = self.N, self.npad, self.gmax
+        run = 0
+        for i in range(Q):                       # the boundary-link grid without padding blocks
+            d.gblock[i] = run
+            run += -(-self.ghosts[i] // 256)
+        d.gblock[Q] = run
         d.gnode, d.ginfo, d.gq = self.gnode.data_ptr(), self.ginfo.data_ptr(), self.gq.data_ptr()
         d.storage = _lib.STORE[self.storage]
         d.model, d.bouzidi, d.gal = self.model, self.bouzidi, self.gal

@@ -205,6 +205,10 @@ typedef struct cs_step_desc {
     double* p_out64;         /* FP64 state of the outlet pressures (n_open) */
     const float* r_out;      /* resistance per open end (n_open) */
     double pref, alpha;
+    /* Boundary-link grid without padding: gblock[i] = sum over directions j < i of ceil(ghosts[j] / 256) (gblock[0] = 0,
+     * gblock[27] = the number of 256-slot blocks over all directions). All zero: the padded grid, ceil(gmax / 256)
+     * blocks for every direction. */
+    int32_t gblock[28];
 } cs_step_desc;
 
 /* Block partition of a sorted flux list for `block` threads per block: out[b] = first entry with
