@@ -216,7 +216,8 @@ typedef struct cs_step_desc {
 int cs_flux_blocks(const int32_t* flux_idx, int64_t n_flux, int64_t n, int32_t block, int32_t* out, void* stream);
 
 /* Enqueue `steps` steps, the first reading buffer a (0/1) and writing 1 - a, alternating (lbm.py:422-428). A step
- * is the boundary-link kernel (when gmax > 0), the bulk kernel and, when n_open > 0, the one-block k_bc kernel. */
+ * is the boundary-link kernel (one block per 256 boundary links of a direction, or a single block without any: it
+ * also advances the clock), the bulk kernel and, when n_open > 0, the one-block k_bc kernel. */
 int cs_step(const cs_step_desc* d, int32_t a, int32_t steps, void* stream);
 
 /* Check a descriptor (HOST struct) as cs_step does, without launching anything. */
