@@ -412,7 +412,7 @@ def main():
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_kind": peak_kind,
                              "traffic": tr * N if tr else None, "bytes_per_update": bplu,
-                             "kernel": "one step = k_boundary + k_bulk (timed together)"},
+                             "kernel": "one step = k_boundary + k_bulk_dense (timed together)"},
                 "back_to_back": {"ms_per_step": b2b * 1e3, "value": world * N / b2b / 1e6, "unit": "MLUPS",
                                  "note": "the same steps in one call without flushing: steady state with L2 reuse"},
                 "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "ok": ok,
