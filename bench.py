@@ -42,7 +42,8 @@ DRIVE = ([0.02, 0.0, 0.01], 4000)       # u0 (1 + 0.5 sin(2 pi t / T)): a0 = 0.0
 BPLU = {"f32": 356, "f16": 248, "bf16": 248}   # algorithmic bytes per lattice update
 METRIC = "D3Q27 MLUPS + HBM GB/s on 1 B200, plain vs batched/FP16; p50/p99 beat latency"
 FLUSH_BYTES = 256 << 20
-TUNED = {"block": 128, "order": "c"}     # launch shape of the batched / served forms (set by the sweep's autotuning)
+# launch shape and batch schedule of the batched / served forms (set by the sweep's autotuning)
+TUNED = {"block": 128, "order": "c", "schedule": "fused"}
 
 
 def nu_lu():
@@ -214,6 +215,10 @@ def bench_sweep(args, dev, peak):
            for sp, lat in zip(specs, lats)]
     nodes = sum(x.N for x in sol)
     b = BatchSolver(sol, block=best["block"])
+    # the schedule (one fused launch over all members per step, or member after member): timed on the batch itself
+    sched, sched_table = autotune.tune_schedule(b, steps=400, chunk=200, warmup=200)
+    TUNED.update(schedule=sched["schedule"])
+    out["autotune"]["schedule"] = {"best": sched["schedule"], "candidates": sched_table}
     b.run(400, chunk=200)
     clocks = Clocks(dev.index)
     secs = timed(lambda: b.run(steps, chunk=200))
@@ -223,7 +228,9 @@ def bench_sweep(args, dev, peak):
     bplu = BPLU[args.sweep_storage]
     out.update({"nodes": nodes, "storage": args.sweep_storage, "value": mlups, "unit": "MLUPS",
                 "hbm_gbs": bplu * mlups / 1e3, "frac": bplu * mlups / 1e3 / peak, "ok": ok,
-                "gpu_launches": 2 * steps, "seconds": secs})
+                "schedule": b.schedule, "seconds": secs,
+                # boundary + bulk per step: once per launch group of 64 (fused), once per member (by-instance)
+                "gpu_launches": 2 * steps * (len(sol) if b.schedule == "by-instance" else -(-len(sol) // 64))})
     del b, sol
     # the plain form: each vessel on its own dedicated FP32 solver, one after another
     tot = 0.0
@@ -248,14 +255,15 @@ def bench_served(args, dev):
 
     specs = W.request_stream(args.serve_requests, seed=5)
     sv = serve.Server(budget_bytes=150e9, storage=args.sweep_storage, steps_per_beat=8000, chunk=1000,
-                      graph_chunk=200, device=dev, keep_fields=True, block=TUNED["block"], order=TUNED["order"])
+                      graph_chunk=200, device=dev, keep_fields=True, block=TUNED["block"], order=TUNED["order"],
+                      schedule=TUNED["schedule"])
     clocks = Clocks(dev.index)
     reqs = sv.serve(specs, realtime=True)
     clk = clocks.stop()
     st = serve.summary(reqs, 8000)
     st["clocks"] = clk
     st.update({"workload": f"first {len(specs)} requests of the seed-5 Poisson stream (2 requests/s)",
-               "storage": args.sweep_storage, "budget_gb": 150.0, "block": TUNED["block"], "order": TUNED["order"],
+               "storage": args.sweep_storage, "budget_gb": 150.0, "block": TUNED["block"], "order": TUNED["order"], "schedule": TUNED["schedule"],
                "max_active": max(n for _, n, _ in sv.trace),
                "peak_reserved_gb": max(u for _, _, u in sv.trace) / 1e9})
     plain = serve.one_by_one(specs, storage="f32", steps_per_beat=8000, device=dev)

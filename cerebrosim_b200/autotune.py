@@ -3,7 +3,8 @@
 For a lattice (or a representative of a batch) each candidate — threads per bulk block x internal node order
 (lbm.node_order: the lattice's C order, C order along the vessel's longest axis, a Morton curve) — is built, warmed
 up and timed with CUDA events over a short run on the solver's stream; the fastest wins. A batch shares one block
-size; the node order is per instance but is chosen once for a family of similar vessels.
+size; the node order is per instance but is chosen once for a family of similar vessels. `tune_schedule` chooses
+a batch's schedule (batch.SCHEDULES: fused launches or instance after instance) the same way, on the batch itself.
 """
 import torch
 
@@ -46,4 +47,25 @@ def tune(lat, nu_lu, configure=None, storage="f32", blocks=BLOCKS, orders=lbm.OR
             table.append({"block": block, "order": order, "us_per_step": sec * 1e6, "mlups": n / sec / 1e6})
             del s
     best = min(table, key=lambda r: r["us_per_step"])
+    return dict(best), table
+
+
+def tune_schedule(batch, steps=400, chunk=200, warmup=200):
+    """Time each batch schedule on `batch` (its members advance `warmup + steps` steps per candidate) and leave the
+    fastest set -> (best, table): best = {"schedule", "us_per_step"}; table = one such dict per schedule. The
+    schedules give the same results, so timing them advances the members as ordinary steps would."""
+    from .batch import SCHEDULES
+    table = []
+    for sch in SCHEDULES:
+        batch.schedule = sch
+        batch.run(warmup, chunk=chunk)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.device(batch.dev):
+            e0.record(batch.stream)
+            batch.run(steps, chunk=chunk)
+            e1.record(batch.stream)
+        batch.synchronize()
+        table.append({"schedule": sch, "us_per_step": e0.elapsed_time(e1) * 1e3 / steps})
+    best = min(table, key=lambda r: r["us_per_step"])
+    batch.schedule = best["schedule"]
     return dict(best), table

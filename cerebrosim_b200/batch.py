@@ -10,6 +10,14 @@ exactly as it would alone.
 
 Instances may join and leave between runs (continuous batching): each keeps its own buffer parity, and the batch
 descriptor table is rebuilt when the membership or an instance's parameters change.
+
+Two schedules advance the members, with the same results (each instance's steps are the same arithmetic on its own
+buffers either way):
+- "fused": every step is one batched launch per kernel over all members (above);
+- "by-instance": each member advances a whole `run` with its own single-lattice kernels and graphs, one member after
+  the other on the batch stream. A member whose working set fits in the L2 then keeps it there from step to step,
+  where the fused launches stream every member's populations through the L2 at every step; on a sweep of 0.3-3 M-node
+  vessels in FP16 this schedule is the faster one. `autotune` chooses between them by measurement.
 """
 import ctypes
 
@@ -20,6 +28,7 @@ from ._lib import check
 from .lbm import ctypes_void
 
 MAX_GROUPS = 64          # launch groups of CS_BATCH_GROUP instances: up to 4096 instances per batch
+SCHEDULES = ("fused", "by-instance")
 
 
 class BatchSolver:
@@ -27,12 +36,15 @@ class BatchSolver:
 
     block: threads per bulk block for every member (their flux partitions are rebuilt to match).
     persistent: size the grids to the GPU (SMs x resident blocks) and loop over work items, instead of one block
-    per work item."""
+    per work item. schedule: "fused" or "by-instance" (module docstring)."""
 
-    def __init__(self, solvers=(), block=128, persistent=True, device=None):
+    def __init__(self, solvers=(), block=128, persistent=True, device=None, schedule="fused"):
+        if schedule not in SCHEDULES:
+            raise ValueError(f"schedule {schedule!r}: one of {SCHEDULES}")
         self.members = []
         self.block = int(block)
         self.persistent = bool(persistent)
+        self.schedule = schedule
         self.dev = None
         self.cur = 0
         self.steps = 0
@@ -111,7 +123,7 @@ class BatchSolver:
         sms = torch.cuda.get_device_properties(self.dev).multi_processor_count
         # the bulk kernel keeps 1024 threads resident per SM (64 registers each): 4 blocks of 256, 8 of 128
         b.grid_bulk = sms * max(1, 1024 // self.block) if self.persistent else 0
-        b.grid_bnd = sms * 8 if self.persistent else 0           # 8 resident boundary blocks per SM
+        b.grid_bnd = sms * 16 if self.persistent else 0          # 16 boundary blocks per SM (2 waves of 8)
         b.descs = ctypes.addressof(self._descs)
         b.parity = ctypes.addressof(self._par)
         b.counter = self._counter.data_ptr()
@@ -133,6 +145,8 @@ class BatchSolver:
         """Advance every member `steps` steps (CUDA graphs of `chunk` batched steps; chunk even)."""
         if not self.members:
             return
+        if self.schedule == "by-instance":
+            return self._run_by_instance(steps, chunk)
         self._refresh()
         lib = _lib.load()
         chunk += chunk % 2
@@ -157,6 +171,18 @@ class BatchSolver:
         for m, p in zip(self.members, self._parity):
             m.cur = self.cur ^ p
             m.steps += int(steps)
+
+    def _run_by_instance(self, steps, chunk):
+        """Each member's `run` in turn with the batch stream current: `Solver.run` makes its own stream wait for
+        the current one and the current one for its own, so the members run one after the other, in order."""
+        self._sync_in()
+        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+            for m in self.members:
+                m.run(steps, chunk=chunk)          # advances m.cur and m.steps itself
+        self._sync_out()
+        self.steps += int(steps)
+        if int(steps) % 2:
+            self.cur = 1 - self.cur
 
     def synchronize(self):
         self.stream.synchronize()

@@ -1069,6 +1069,17 @@ __global__ void __launch_bounds__(MAX_BLOCK, MIN_BLOCKS) k_bulk_batch(const __gr
     }
 }
 
+// One block per bulk item, no loop and no claims (grid_bulk = 0): the regularised step without body force in blocks
+// of at most 128 threads, compiled like k_bulk_dense for 9 blocks per SM, which the persistent loop's state does not
+// leave registers for. The block finds its instance by a binary search over the item prefix in the parameters.
+template <int ST, bool GAL>
+__global__ void __launch_bounds__(DENSE_BLOCK, DENSE_MIN_BLOCKS) k_bulk_batch_dense(const __grid_constant__ BatchGroup g,
+                                                                                  const int a) {
+    const int item = int(blockIdx.x);
+    const int inst = find_instance(g.bulk_prefix, g.n_inst, item);
+    bulk_body<ST, CS_MODEL_REGULARISED, GAL, false>(g.d[inst], a ^ g.parity[inst], item - g.bulk_prefix[inst]);
+}
+
 __global__ void k_bc_batch(const __grid_constant__ BatchGroup g) {
     const cs_step_desc& d = g.d[blockIdx.x];
     if (d.n_open > 0) bc_body(d);
@@ -1077,7 +1088,9 @@ __global__ void k_bc_batch(const __grid_constant__ BatchGroup g) {
 using BatchFn = void (*)(const BatchGroup, const int);
 
 template <int ST>
-BatchFn pick_batch_model(int model, int gal, bool force) {
+BatchFn pick_batch_model(int model, int gal, bool force, bool dense) {
+    if (dense && model == CS_MODEL_REGULARISED && !force)
+        return gal ? k_bulk_batch_dense<ST, true> : k_bulk_batch_dense<ST, false>;
     if (model == CS_MODEL_REGULARISED) {
         if (gal) return force ? k_bulk_batch<ST, CS_MODEL_REGULARISED, true, true> : k_bulk_batch<ST, CS_MODEL_REGULARISED, true, false>;
         return force ? k_bulk_batch<ST, CS_MODEL_REGULARISED, false, true> : k_bulk_batch<ST, CS_MODEL_REGULARISED, false, false>;
@@ -1162,9 +1175,10 @@ int launch_batch_pdl(BatchFn fn, unsigned grid, unsigned block, cudaStream_t st,
 int launch_batch(const cs_batch_desc* b, int a, int steps, cudaStream_t st) {
     const std::vector<BatchGroup> gs = make_groups(b);
     const bool force = b->force != 0;
-    BatchFn bulk = b->storage == CS_STORE_F16    ? pick_batch_model<CS_STORE_F16>(b->model, b->gal, force)
-                   : b->storage == CS_STORE_BF16 ? pick_batch_model<CS_STORE_BF16>(b->model, b->gal, force)
-                                                 : pick_batch_model<CS_STORE_F32>(b->model, b->gal, force);
+    const bool dense = b->grid_bulk == 0 && b->block <= DENSE_BLOCK;     // one block per item: k_bulk_batch_dense
+    BatchFn bulk = b->storage == CS_STORE_F16    ? pick_batch_model<CS_STORE_F16>(b->model, b->gal, force, dense)
+                   : b->storage == CS_STORE_BF16 ? pick_batch_model<CS_STORE_BF16>(b->model, b->gal, force, dense)
+                                                 : pick_batch_model<CS_STORE_F32>(b->model, b->gal, force, dense);
     BatchFn bound = b->storage == CS_STORE_F16    ? k_boundary_batch<CS_STORE_F16>
                     : b->storage == CS_STORE_BF16 ? k_boundary_batch<CS_STORE_BF16>
                                                   : k_boundary_batch<CS_STORE_F32>;

@@ -77,13 +77,14 @@ class Server:
     budget_bytes: device memory the resident requests may hold (admission control); max_active: largest batch;
     chunk: steps per scheduling round (a divisor of steps_per_beat); graph_chunk: steps per captured graph;
     ahead: chunks kept enqueued; keep_fields: read each result's (p, u) back to the host; block and order: the
-    launch shape and node order of every request's solver (autotune.tune picks them); on_beat(request, beat): called
+    launch shape and node order of every request's solver (autotune.tune picks them); schedule: the batch's schedule
+    (batch.SCHEDULES; autotune.tune_schedule picks it); on_beat(request, beat): called
     when a request completes a beat (not its last), with its solver's state final for that beat — what it changes
     (a recalibrated drive: simulate.recalibrate) applies from the next beat's first step."""
 
     def __init__(self, budget_bytes=150e9, storage="bf16", steps_per_beat=8000, chunk=1000, graph_chunk=200,
                  max_active=64, block=128, ahead=2, keep_fields=True, device=None, builder=default_builder,
-                 order="c", on_beat=None):
+                 order="c", on_beat=None, schedule="fused"):
         if steps_per_beat % chunk or chunk % 2 or graph_chunk % 2:
             raise ValueError("chunk must divide steps_per_beat; chunk and graph_chunk must be even")
         self.budget = float(budget_bytes)
@@ -99,6 +100,7 @@ class Server:
         self.builder = builder
         self.order = order
         self.on_beat = on_beat
+        self.schedule = schedule
         self.trace = []         # (seconds, active requests, reserved bytes) after each admission
 
     def estimate(self, spec):
@@ -181,7 +183,7 @@ class Server:
                     break
                 queue.popleft()
                 if batch is None:
-                    batch = BatchSolver(block=self.block)
+                    batch = BatchSolver(block=self.block, schedule=self.schedule)
                 self._admit(r, batch, t0)
                 if start is None:
                     start = torch.cuda.Event(enable_timing=True)

@@ -5,6 +5,10 @@
   without atomics), whatever the mix and whenever instances join or leave.
 - Batched and dedicated kernels: the batched kernels and the single-lattice kernels are compiled separately and
   may round differently in the last bit; they agree within the path's tolerance, relative L2 <= 1e-5.
+- Both batched forms: the persistent grid (blocks claim work items) and one block per work item (the 9-blocks-per-SM
+  kernel of the regularised step without body force).
+- The by-instance schedule runs each member with its own single-lattice kernels: bit for bit the member's solo run,
+  joins and leaves included, and within 1e-5 of the fused schedule.
 """
 import numpy as np
 import pytest
@@ -79,32 +83,34 @@ def close(a, b, tol=1e-5):
     assert a.tick_value() == b.tick_value()
 
 
-def run_alone(s, steps, chunk):
+def run_alone(s, steps, chunk, persistent=True):
     """An instance in a batch of its own."""
-    b = BatchSolver([s])
+    b = BatchSolver([s], persistent=persistent)
     b.run(steps, chunk=chunk)
     return b
 
 
+@pytest.mark.parametrize("persistent", [True, False])
 @pytest.mark.parametrize("storage", ["f32", "bf16"])
-def test_batch_alone_and_in_the_mix(golden, storage):
+def test_batch_alone_and_in_the_mix(golden, storage, persistent):
     alone = [make(golden, n, c, k, storage) for n, c, k in SPECS]
     mixed = [make(golden, n, c, k, storage) for n, c, k in SPECS]
     for s in alone:
-        run_alone(s, 501, 100)
-    b = BatchSolver(mixed)
+        run_alone(s, 501, 100, persistent)
+    b = BatchSolver(mixed, persistent=persistent)
     b.run(501, chunk=100)
     assert b.steps == 501 and all(m.steps == 501 for m in mixed)
     for a, m in zip(alone, mixed):
         same(a, m)
 
 
-def test_batched_kernels_match_dedicated_kernels(golden):
+@pytest.mark.parametrize("persistent", [True, False])
+def test_batched_kernels_match_dedicated_kernels(golden, persistent):
     dedicated = [make(golden, n, c, k) for n, c, k in SPECS]
     batched = [make(golden, n, c, k) for n, c, k in SPECS]
     for s in dedicated:
         s.run(501, chunk=100)
-    BatchSolver(batched).run(501, chunk=100)
+    BatchSolver(batched, persistent=persistent).run(501, chunk=100)
     for a, m in zip(dedicated, batched):
         close(a, m)
 
@@ -126,6 +132,32 @@ def test_batch_members_join_and_leave(golden):
         run_alone(s, k, 40)
     for a, m in zip(alone, mixed):
         same(a, m)
+
+
+def test_by_instance_schedule_is_the_solo_run(golden):
+    solo = [make(golden, n, c, k) for n, c, k in SPECS]
+    mixed = [make(golden, n, c, k) for n, c, k in SPECS]
+    fused = [make(golden, n, c, k) for n, c, k in SPECS]
+    b = BatchSolver(mixed[:3], schedule="by-instance")
+    b.run(101, chunk=40)
+    b.remove(mixed[1])
+    b.add(mixed[3])
+    b.run(60, chunk=40)
+    steps = [161, 101, 161, 60]
+    for s, k in zip(solo, steps):
+        s.block = 128            # the batch's block size, which the members take on joining
+        if hasattr(s, "_set_flux_blocks"):
+            s._set_flux_blocks()
+        s.run(k, chunk=40)
+    for a, m in zip(solo, mixed):
+        same(a, m)
+    bf = BatchSolver(fused[:3])
+    bf.run(101, chunk=40)
+    bf.remove(fused[1])
+    bf.add(fused[3])
+    bf.run(60, chunk=40)
+    for a, m in zip(fused, mixed):
+        close(a, m)
 
 
 def test_coupled_runs_are_reproducible(golden):

@@ -35,9 +35,10 @@ def l2(a, b):
     return float(np.sqrt(((a.astype(np.float64) - b) ** 2).sum() / max((b.astype(np.float64) ** 2).sum(), 1e-300)))
 
 
+@pytest.mark.parametrize("schedule", ["fused", "by-instance"])
 @pytest.mark.parametrize("storage", ["f32", "bf16"])
-def test_served_results_same_alone_and_in_the_mix(storage):
-    sv = server(storage, max_active=3)
+def test_served_results_same_alone_and_in_the_mix(storage, schedule):
+    sv = server(storage, max_active=3, schedule=schedule)
     mix = sv.serve(specs(), realtime=False)
     assert all(r.ok for r in mix)
     # the mix really overlapped: up to three requests shared the launches, later ones joined mid-run
@@ -45,15 +46,16 @@ def test_served_results_same_alone_and_in_the_mix(storage):
     assert max(r.queue_wait for r in mix) > 0
     for r in mix:
         assert len(r.beat_end) == r.beats and len(r.beat_latencies()) == r.beats
-        alone = server(storage).serve([r.spec], realtime=False)[0]
+        alone = server(storage, schedule=schedule).serve([r.spec], realtime=False)[0]
         p0, u0 = alone.fields
         p1, u1 = r.fields
         assert np.array_equal(p0, p1) and np.array_equal(u0, u1), r.id
 
 
-def test_served_matches_dedicated_solver():
+@pytest.mark.parametrize("schedule", ["fused", "by-instance"])
+def test_served_matches_dedicated_solver(schedule):
     sp = specs()[0]
-    r = server("f32", max_active=3).serve(specs(), realtime=False)[0]
+    r = server("f32", max_active=3, schedule=schedule).serve(specs(), realtime=False)[0]
     s = serve.default_builder(sp, "f32", 256, None, SPB)
     s.run(sp["beats"] * SPB, chunk=50)
     p, u = s.fields()
