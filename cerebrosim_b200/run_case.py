@@ -57,7 +57,7 @@ def main():
         from . import workloads
         spec = {"seed": a.artery, "stenosis": 0.7, "pressure": 95.0}
         lat = workloads.lattice(workloads.stenosed_vessel(a.artery), a.dx)
-        s = workloads.make_solver(spec, lat, storage=a.storage, block=a.block or 256)
+        s = workloads.make_solver(spec, lat, storage=a.storage, block=a.block)
         a.case = f"artery_seed{a.artery}_dx{a.dx}"
     else:
         s = make_solver(a.case, a.storage, a.block)
