@@ -160,6 +160,18 @@ def test_by_instance_schedule_is_the_solo_run(golden):
         close(a, m)
 
 
+def test_schedule_tuning_times_both_and_keeps_the_faster(golden):
+    from cerebrosim_b200 import autotune
+    from cerebrosim_b200.batch import SCHEDULES
+    members = [make(golden, n, c, k) for n, c, k in SPECS[:2]]
+    b = BatchSolver(members)
+    best, table = autotune.tune_schedule(b, steps=20, chunk=10, warmup=10)
+    assert [r["schedule"] for r in table] == list(SCHEDULES)
+    assert best["schedule"] == b.schedule == min(table, key=lambda r: r["us_per_step"])["schedule"]
+    assert all(r["us_per_step"] > 0 for r in table)
+    assert b.steps == 60 and all(m.steps == 60 and m.ok() for m in members)
+
+
 def test_coupled_runs_are_reproducible(golden):
     """The resistance coupling reduces its flux without atomics: two runs agree bit for bit."""
     n, c, k = SPECS[3]
