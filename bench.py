@@ -310,7 +310,7 @@ def main():
     # order (the split order gains ~3 % back to back but nothing with a cold L2, and costs the end-to-end path its
     # renumbering)
     from cerebrosim_b200 import autotune
-    tuned, tune_table = autotune.tune(lat, nu_lu(), configure=configure, storage=args.storage, blocks=(128, 256),
+    tuned, tune_table = autotune.tune(lat, nu_lu(), configure=configure, storage=args.storage, blocks=(64, 128, 256),
                                       orders=("c",), steps=400, warmup=100, device=dev, model="regularised")
     shape = {"block": tuned["block"], "order": tuned["order"]}
     s = lbm.Solver(lat, nu_lu(), model="regularised", device=dev, storage=args.storage, **shape)

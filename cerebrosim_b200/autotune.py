@@ -10,7 +10,7 @@ import torch
 
 from . import lbm
 
-BLOCKS = (128, 192, 256)
+BLOCKS = (64, 128, 192, 256)
 
 
 def time_steps(s, steps, warmup):

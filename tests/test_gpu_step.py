@@ -89,6 +89,30 @@ def test_open_pipe_inlet_outlet_sponge(golden, model, sigma, gal, bouzidi):
     compare(g, r)
 
 
+def test_block_sizes_agree(golden):
+    """Every bulk block size gives the oracle's fields; the sizes of at most 128 threads run one build of the kernel
+    (9 blocks of 128 per SM) and agree bit for bit."""
+    lg, lr = lattice_from_golden(golden, "open_pipe_tilted_R4")
+
+    def setup(s):
+        s.set_sponge(4, 0.6)
+        s.set_drive([0.02, 0.004, -0.003], period=300, ramp=150)
+        s.set_outlet_pressure([1e-4])
+    r = OracleSolver(lr, 0.02, model="regularised")
+    setup(r)
+    r.run(STEPS)
+    dense = []
+    for block in (32, 64, 96, 128, 192, 256):
+        g = lbm.Solver(lg, 0.02, model="regularised", block=block)
+        setup(g)
+        g.run(STEPS)
+        compare(g, r)
+        if block <= 128:
+            dense.append(g.fields())
+    for p, u in dense[1:]:
+        assert np.array_equal(p, dense[0][0]) and np.array_equal(u, dense[0][1])
+
+
 def test_stenosis_small(golden):
     lg, lr = lattice_from_golden(golden, "stenosis70_D8")
 
