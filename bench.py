@@ -69,9 +69,14 @@ def configure(s):
 
 
 def measured_peak():
+    """The pod's measured copy bandwidth (GB/s) when MEASURED_PEAKS.json holds one, else the pool's fallback."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(p):
-        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    try:
+        v = float(json.load(open(p))["hbm_gbs"])
+        if v > 0:
+            return v, "measured"
+    except (OSError, ValueError, KeyError, TypeError):
+        pass
     return 6650.0, "fallback"
 
 
