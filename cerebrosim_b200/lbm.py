@@ -7,9 +7,10 @@ State lives in PyTorch CUDA tensors; every step is one hand-written sm_100a kern
 are CUDA graphs, as in the reference. There is no CPU path: without a CUDA device or the library, construction
 raises.
 
-Differences a caller can see (all documented in DESIGN.md):
+Differences a caller can see:
   - only D3Q27 (the reference's default; ARTERY_LBM_LATTICE=D3Q19 raises ValueError);
-  - `Solver(..., storage="f32" | "f16" | "bf16", block=None)`: population storage format and threads per block;
+  - `Solver(..., storage="f32" | "f16" | "bf16", block=None, order="c")`: population storage format, threads per
+    block and the internal node order (fields are returned in the lattice's order whatever it is);
   - `vels[k]` is an (N, 3) view of a (3, N) structure-of-arrays buffer; `fields()` returns NumPy copies as before.
 """
 import ctypes
@@ -23,7 +24,7 @@ from ._lib import check
 
 LATTICE = os.environ.get("ARTERY_LBM_LATTICE", "D3Q27")
 if LATTICE != "D3Q27":
-    raise ValueError(f"ARTERY_LBM_LATTICE={LATTICE}: this build implements D3Q27 only")
+    raise ValueError(f"ARTERY_LBM_LATTICE={LATTICE}: this package implements D3Q27 only")
 
 # lbm.py:34-47
 C = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1],
