@@ -3,7 +3,7 @@
  * The reference (CerebroSim) is pure Python: its solver interface is `lbm.py` (module functions + class Solver)
  * and `simulate.py`'s `ArterySolver`; it has no FFI of its own. Each entry point below names the reference
  * function or kernel whose behaviour it provides; the Python package `cerebrosim_b200` binds them with ctypes
- *  behind the same `lbm` / `Solver` interface.
+ * (cerebrosim_b200/_lib.py) behind the same `lbm` / `Solver` interface.
  *
  * Conventions
  *  - Every function returns an int status: CS_OK (0) or a CS_ERR_* code; cs_last_error() gives the message of the
