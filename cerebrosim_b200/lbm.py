@@ -399,9 +399,15 @@ class Solver:
                     self.graphs[key] = self._capture(self.cur, chunk)
                 for _ in range(full):
                     self._replay(self.graphs[key])
-            for _ in range(rest):
-                self._launch(self.cur)
-                self.cur = 1 - self.cur
+            if rest and type(self)._launch is Solver._launch:
+                # the leftover steps in one library call (the same launches, without a descriptor per step)
+                check(_lib.load().cs_step(ctypes.byref(self._desc()), int(self.cur), int(rest),
+                                          ctypes_void(self.stream.cuda_stream)))
+                self.cur ^= rest & 1
+            else:
+                for _ in range(rest):
+                    self._launch(self.cur)
+                    self.cur = 1 - self.cur
         cur_stream.wait_stream(self.stream)
         self.steps += int(steps)
 

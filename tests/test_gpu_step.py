@@ -174,7 +174,8 @@ def test_graph_and_single_launches_identical(golden):
     lg, _ = lattice_from_golden(golden, "open_pipe_straight_R4")
     a = lbm.Solver(lg, 0.02, model="regularised")
     b = lbm.Solver(lg, 0.02, model="regularised")
-    for s in (a, b):
+    c = lbm.Solver(lg, 0.02, model="regularised")
+    for s in (a, b, c):
         s.set_sponge(4, 0.6)
         s.set_drive([0.02], ramp=100)
     a.run(1001, chunk=100)
@@ -182,11 +183,14 @@ def test_graph_and_single_launches_identical(golden):
         b._launch(b.cur)
         b.cur = 1 - b.cur
     b.steps = 1001
+    c.run(1001, chunk=2000)          # no full chunk: the 1001 leftover steps in one library call
     pa, ua = a.fields()
     pb, ub = b.fields()
-    assert a.cur == b.cur == 1
+    pc, uc = c.fields()
+    assert a.cur == b.cur == c.cur == 1 and c.steps == 1001 and c.tick_value() == b.tick_value()
     assert np.array_equal(pa, pb) and np.array_equal(ua, ub)
-    assert torch.equal(a.f[a.cur], b.f[b.cur])
+    assert np.array_equal(pc, pb) and np.array_equal(uc, ub)
+    assert torch.equal(a.f[a.cur], b.f[b.cur]) and torch.equal(c.f[c.cur], b.f[b.cur])
 
 
 def test_subclass_launch_hook_is_captured(golden):
