@@ -433,12 +433,15 @@ class Solver:
         """(pressure, velocity) per cell of the lattice (its node order, whatever the internal one), lattice units,
         as NumPy (lbm.py:450-452)."""
         self.stream.synchronize()
-        rho, vel = self.rho, self.vel[self.cur]
-        if self.inv is not None:
-            with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+            rho, vel = self.rho, self.vel[self.cur]
+            if self.inv is not None:
                 rho, vel = rho[self.inv], vel[:, self.inv]
-            self.stream.synchronize()
-        return rho.cpu().numpy() / 3.0, np.ascontiguousarray(vel.cpu().numpy().T)
+            # the (3, N) buffer transposed on the device: the read-back is one contiguous copy, not a strided one on
+            # the host; p = rho / 3 stays a host division, as the reference's
+            u = vel.t().contiguous().cpu().numpy()
+            p = rho.cpu().numpy()
+        return p / 3.0, u
 
     def ok(self):
         """All densities finite (lbm.py:454-455)."""
