@@ -62,6 +62,26 @@ def test_periodic_pipe_body_force():
     compare(g, r)
 
 
+def test_headline_pipe_at_full_size():
+    """The bench's workload itself — the open pipe R = 24, L = 192 (347,328 nodes) with the plug inlet, its Fourier
+    drive and the pressure outlet, tau 0.55 — for 300 steps against the oracle on the same tables."""
+    from cerebrosim_b200 import run_case
+    c = cases.case("open_pipe_R24_L192")
+    lg = run_case.plug_inlet(lbm.build_lattice(**cases.lattice_args(c)))
+    lr = run_case.plug_inlet(L.build_lattice(**cases.lattice_args(c)))
+    assert lg["nbr"].shape[1] == 347328
+    for k in ("nbr", "q", "uin"):
+        assert np.array_equal(lg[k], lr[k]), k
+
+    def setup(s):
+        s.set_drive([0.02, 0.0, 0.01], period=4000)
+        s.set_outlet_pressure([0.0])
+    g, r = both(lg, lr, (0.55 - 0.5) / 3.0, setup, model="regularised")
+    for s in (g, r):
+        s.run(300)
+    compare(g, r)
+
+
 def test_poiseuille_cylinder_tau08():
     """The small Poiseuille cylinder: R = 10, 24 x 24 x 64 periodic, tau = 0.8, g = 1e-6."""
     c = cases.case("poiseuille_R10_L64")
