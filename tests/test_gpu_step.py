@@ -82,6 +82,26 @@ def test_headline_pipe_at_full_size():
     compare(g, r)
 
 
+@pytest.mark.parametrize("storage,bound", [("f16", 3e-3), ("bf16", 3e-2)])
+def test_headline_pipe_16bit_at_full_size(storage, bound):
+    """The bench's 347,328-node pipe with 16-bit shifted storage, 300 steps, against the FP64 oracle of the same
+    scheme: the bounds of the small-lattice 16-bit check hold at full size."""
+    from cerebrosim_b200 import run_case
+    c = cases.case("open_pipe_R24_L192")
+    lg = run_case.plug_inlet(lbm.build_lattice(**cases.lattice_args(c)))
+    lr = run_case.plug_inlet(L.build_lattice(**cases.lattice_args(c)))
+    g = lbm.Solver(lg, (0.55 - 0.5) / 3.0, model="regularised", storage=storage)
+    r = OracleSolver(lr, (0.55 - 0.5) / 3.0, model="regularised", dtype=np.float64)
+    for s in (g, r):
+        s.set_drive([0.02, 0.0, 0.01], period=4000)
+        s.set_outlet_pressure([0.0])
+        s.run(300)
+    _, u_g = g.fields()
+    _, u_r = r.fields()
+    assert g.ok()
+    assert rel_l2(u_g.astype(np.float64), u_r) <= bound
+
+
 def test_poiseuille_cylinder_tau08():
     """The small Poiseuille cylinder: R = 10, 24 x 24 x 64 periodic, tau = 0.8, g = 1e-6."""
     c = cases.case("poiseuille_R10_L64")
