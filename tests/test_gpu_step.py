@@ -102,6 +102,23 @@ def test_headline_pipe_16bit_at_full_size(storage, bound):
     assert rel_l2(u_g.astype(np.float64), u_r) <= bound
 
 
+def test_stenosed_artery_at_full_size():
+    """The batched / served workloads' vessel at its full size: the generated stenosed artery of seed 3 at 0.05 mm
+    (1,567,027 nodes; Bouzidi walls, Fourier velocity inlet, two pressure outlets, sponge), 100 FP32 steps against
+    the oracle on the same tables, in the lattice's C order and in the vessel-axis order the autotuner picks."""
+    from cerebrosim_b200 import workloads
+    spec = {"seed": 3, "stenosis": 0.7, "pressure": 95.0}
+    lat = workloads.lattice(workloads.stenosed_vessel(3), 0.05)
+    assert lat["nbr"].shape[1] == 1567027
+    r = OracleSolver(lat, (0.52 - 0.5) / 3.0, model="regularised")
+    workloads.configure(r, spec, lat, period=8000)
+    r.run(100)
+    for order in ("c", "axis-split"):
+        g = workloads.make_solver(spec, lat, period=8000, order=order)
+        g.run(100)
+        compare(g, r)
+
+
 def test_poiseuille_cylinder_tau08():
     """The small Poiseuille cylinder: R = 10, 24 x 24 x 64 periodic, tau = 0.8, g = 1e-6."""
     c = cases.case("poiseuille_R10_L64")
