@@ -50,19 +50,6 @@ def nu_lu():
     return (TAU - 0.5) / 3.0
 
 
-def plug_inlet(lat):
-    """Replace the builder's parabolic inlet profile by a plug of unit speed along the inward normal."""
-    import torch
-    inlet = [o for o in lat["openings"] if o["kind"] == "inlet"][-1]
-    cells = (lat["nbr"] == -2).any(0)
-    uin = np.zeros_like(lat["uin"])
-    uin[cells] = (-np.asarray(inlet["normal"], float)).astype(np.float32)
-    lat["uin"] = uin
-    if "_dev" in lat:
-        lat["_dev"]["uin"] = torch.as_tensor(uin).to(lat["_dev"]["nbr"].device)
-    return lat
-
-
 def configure(s):
     s.set_drive(DRIVE[0], period=DRIVE[1])
     s.set_outlet_pressure([0.0])
@@ -156,7 +143,7 @@ def run_reference(args):
     from cerebrosim_b200 import cases
     from oracle import lattice_ref as L
     from oracle.step_ref import OracleSolver
-    lat = plug_inlet(L.build_lattice(**cases.lattice_args(cases.case(WORKLOAD))))
+    lat = cases.plug_inlet(L.build_lattice(**cases.lattice_args(cases.case(WORKLOAD))))
     N = lat["nbr"].shape[1]
     s = OracleSolver(lat, nu_lu(), model="regularised")
     configure(s)
@@ -309,7 +296,7 @@ def main():
     barrier, max_over_ranks = rep.barrier, rep.max
 
     c = cases.case(WORKLOAD)
-    lat = plug_inlet(lbm.build_lattice(**cases.lattice_args(c), device=dev))
+    lat = cases.plug_inlet(lbm.build_lattice(**cases.lattice_args(c), device=dev))
     N = lat["nbr"].shape[1]
     # block size chosen by the autotuner (short timed runs of each candidate on this lattice); the reference's node
     # order (the split order gains ~3 % back to back but nothing with a cold L2, and costs the end-to-end path its
@@ -438,7 +425,7 @@ def main():
             line["served"] = bench_served(args, dev)
         if world == 1 and not args.no_cpu_baseline:
             from oracle import lattice_ref as L
-            line["cpu_baseline"] = cpu_baseline(plug_inlet(L.build_lattice(**cases.lattice_args(c))))
+            line["cpu_baseline"] = cpu_baseline(cases.plug_inlet(L.build_lattice(**cases.lattice_args(c))))
         print(json.dumps(line), flush=True)
     rep.close()
 

@@ -55,3 +55,17 @@ def case(name):
 def lattice_args(c):
     """The keyword arguments of build_lattice from a case dict."""
     return {k: c[k] for k in ("phi", "origin", "dx", "openings", "periodic")}
+
+
+def plug_inlet(lat):
+    """Replace the builder's parabolic inlet profile by a plug of unit speed along the inward normal of the last
+    inlet (the pulsatile pipe's inflow: the drive then scales it to u0 (1 + 0.5 sin(2 pi t / T)))."""
+    inlet = [o for o in lat["openings"] if o["kind"] == "inlet"][-1]
+    cells = (np.asarray(lat["nbr"]) == -2).any(0)
+    uin = np.zeros_like(np.asarray(lat["uin"]))
+    uin[cells] = (-np.asarray(inlet["normal"], float)).astype(np.float32)
+    lat["uin"] = uin
+    if "_dev" in lat:
+        import torch
+        lat["_dev"]["uin"] = torch.as_tensor(uin).to(lat["_dev"]["nbr"].device)
+    return lat

@@ -237,26 +237,16 @@ constexpr int64_t NOALLOC_WORDS = int64_t(Q) * (NOALLOC_TILES + 1) + 2;    // ti
 
 static __device__ __align__(256) int64_t g_noalloc_scratch[NOALLOC_WORDS];
 
-constexpr int MAX_DEVICES = 64;
-std::mutex g_noalloc_mu;
-int64_t* g_noalloc_ptr[MAX_DEVICES] = {};
-
 // Device address of the static scratch on the current device. The host-side name g_noalloc_scratch is only a
-// stand-in for the symbol, never a device address, so the address is looked up once per device (with that device
-// current) and cached.
+// stand-in for the symbol, never a device address, so the address is looked up with the device current. It is
+// looked up on every call rather than cached: a cached address would go stale if the caller reset the device
+// (cudaDeviceReset) and a new context placed the array elsewhere.
 int noalloc_scratch(int64_t** out) {
-    int dev = 0;
-    CS_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= MAX_DEVICES) return fail(CS_ERR_SIZE, "cs_links_build_noalloc: device %d", dev);
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return fail(CS_ERR_CUDA, "cs_links_build_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
-        g_noalloc_ptr[dev] = static_cast<int64_t*>(p);
-    }
-    *out = g_noalloc_ptr[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return fail(CS_ERR_CUDA, "cs_links_build_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+    *out = static_cast<int64_t*>(p);
     return CS_OK;
 }
 

@@ -136,10 +136,10 @@ int cs_links_fill(const int32_t* nbr, const float* q, int64_t n, int32_t n_out, 
  * for gmax_cap ghost slots per direction (tables 27 * gmax_cap, gnode pre-filled with -1 so that unused slots are
  * marked); ghosts (HOST, 27 int64) receives the counts, and CS_ERR_SIZE comes back (with the counts) when a
  * direction needs more than gmax_cap. The ghost tables then have stride gmax_cap: use it as gmax in the step.
- * The first call on a device looks up the array's device address (with that device current) and caches it; make
- * that first call before any stream capture. Every call shares the one array and resets what it reads before
- * reading it, but calls that overlap on the GPU (other streams, other host threads) race on it. Synchronises
- * `stream`; makes no cudaMalloc, cudaFree or other allocating call. */
+ * Each call looks up the array's device address on the current device. Every call shares the one array and resets
+ * what it reads before reading it, but calls that overlap on the GPU (other streams, other host threads) race on
+ * it. Synchronises `stream` (twice: to read the counts, then the status); makes no cudaMalloc, cudaFree or other
+ * allocating call. */
 int cs_links_build_noalloc(const int32_t* nbr, const float* q, int64_t n, int32_t n_out, int64_t gmax_cap,
                            int32_t* links, int32_t* gnode, int32_t* ginfo, float* gq, int64_t* ghosts, void* stream);
 

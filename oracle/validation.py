@@ -11,7 +11,7 @@ import time
 
 import numpy as np
 
-from . import cases
+from cerebrosim_b200 import cases
 
 RHO = 1060.0                     # kg/m^3 (vessel.py:49)
 MU = 3.5e-3                      # Pa s (vessel.py:50)

@@ -65,10 +65,9 @@ def test_periodic_pipe_body_force():
 def test_headline_pipe_at_full_size():
     """The bench's workload itself — the open pipe R = 24, L = 192 (347,328 nodes) with the plug inlet, its Fourier
     drive and the pressure outlet, tau 0.55 — for 300 steps against the oracle on the same tables."""
-    from cerebrosim_b200 import run_case
     c = cases.case("open_pipe_R24_L192")
-    lg = run_case.plug_inlet(lbm.build_lattice(**cases.lattice_args(c)))
-    lr = run_case.plug_inlet(L.build_lattice(**cases.lattice_args(c)))
+    lg = cases.plug_inlet(lbm.build_lattice(**cases.lattice_args(c)))
+    lr = cases.plug_inlet(L.build_lattice(**cases.lattice_args(c)))
     assert lg["nbr"].shape[1] == 347328
     for k in ("nbr", "q", "uin"):
         assert np.array_equal(lg[k], lr[k]), k
@@ -86,10 +85,9 @@ def test_headline_pipe_at_full_size():
 def test_headline_pipe_16bit_at_full_size(storage, bound):
     """The bench's 347,328-node pipe with 16-bit shifted storage, 300 steps, against the FP64 oracle of the same
     scheme: the bounds of the small-lattice 16-bit check hold at full size."""
-    from cerebrosim_b200 import run_case
     c = cases.case("open_pipe_R24_L192")
-    lg = run_case.plug_inlet(lbm.build_lattice(**cases.lattice_args(c)))
-    lr = run_case.plug_inlet(L.build_lattice(**cases.lattice_args(c)))
+    lg = cases.plug_inlet(lbm.build_lattice(**cases.lattice_args(c)))
+    lr = cases.plug_inlet(L.build_lattice(**cases.lattice_args(c)))
     g = lbm.Solver(lg, (0.55 - 0.5) / 3.0, model="regularised", storage=storage)
     r = OracleSolver(lr, (0.55 - 0.5) / 3.0, model="regularised", dtype=np.float64)
     for s in (g, r):

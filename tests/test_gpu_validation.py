@@ -13,7 +13,8 @@ import torch
 
 pytestmark = pytest.mark.gpu
 
-from cerebrosim_b200 import lbm, validation as V  # noqa: E402
+from cerebrosim_b200 import lbm  # noqa: E402
+from oracle import validation as V  # noqa: E402
 
 P = V.PUBLISHED
 

@@ -7,7 +7,7 @@ contraction (as the reference's GPU compiler does) the FP32 restatement reproduc
 import numpy as np
 import pytest
 
-from cerebrosim_b200 import validation as V
+from oracle import validation as V
 from oracle import lattice_ref as L
 from oracle.step_ref import OracleSolver
 
