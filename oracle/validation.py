@@ -86,6 +86,16 @@ def womersley_exact(r, R, Wo, F0, w, t):
     return np.real(U * np.exp(1j * w * t))
 
 
+def womersley_flow(r, R, Wo, U_hat, w, t):
+    """Oscillatory pipe flow of prescribed cross-section mean velocity Re{U_hat e^(i w t)} (the textbook Womersley
+    solution written for a flow rate instead of a pressure gradient): Re{U_hat (1 - J0(k r / R) / J0(k)) /
+    (1 - 2 J1(k) / (k J0(k))) e^(i w t)}, k = i^(3/2) Wo. The pressure-driven form above has the same shape."""
+    from scipy.special import jv
+    k = (1j ** 1.5) * Wo
+    shape = (1 - jv(0, k * r / R) / jv(0, k)) / (1 - 2 * jv(1, k) / (k * jv(0, k)))
+    return np.real(U_hat * shape * np.exp(1j * w * t))
+
+
 def womersley(build, make, Wo, D=20, phases=12, nu=None):
     """Pulsatile pipe flow: L2 error over 12 phases of the third period against the Bessel solution."""
     nu = units("healthy").nu_lu if nu is None else nu

@@ -63,8 +63,9 @@ def test_periodic_pipe_body_force():
 
 
 def test_headline_pipe_at_full_size():
-    """The bench's workload itself — the open pipe R = 24, L = 192 (347,328 nodes) with the plug inlet, its Fourier
-    drive and the pressure outlet, tau 0.55 — for 300 steps against the oracle on the same tables."""
+    """The bench's workload itself — the pulsatile pipe: open pipe R = 24, L = 192 (347,328 nodes) with the plug
+    inlet, its Fourier drive and the pressure outlet, tau 0.55 — for 1000 steps against the oracle on the same
+    tables."""
     c = cases.case("open_pipe_R24_L192")
     lg = cases.plug_inlet(lbm.build_lattice(**cases.lattice_args(c)))
     lr = cases.plug_inlet(L.build_lattice(**cases.lattice_args(c)))
@@ -77,7 +78,7 @@ def test_headline_pipe_at_full_size():
         s.set_outlet_pressure([0.0])
     g, r = both(lg, lr, (0.55 - 0.5) / 3.0, setup, model="regularised")
     for s in (g, r):
-        s.run(300)
+        s.run(STEPS)
     compare(g, r)
 
 
@@ -102,7 +103,7 @@ def test_headline_pipe_16bit_at_full_size(storage, bound):
 
 def test_stenosed_artery_at_full_size():
     """The batched / served workloads' vessel at its full size: the generated stenosed artery of seed 3 at 0.05 mm
-    (1,567,027 nodes; Bouzidi walls, Fourier velocity inlet, two pressure outlets, sponge), 100 FP32 steps against
+    (1,567,027 nodes; Bouzidi walls, Fourier velocity inlet, two pressure outlets, sponge), 1000 FP32 steps against
     the oracle on the same tables, in the lattice's C order and in the vessel-axis order the autotuner picks."""
     from cerebrosim_b200 import workloads
     spec = {"seed": 3, "stenosis": 0.7, "pressure": 95.0}
@@ -110,10 +111,10 @@ def test_stenosed_artery_at_full_size():
     assert lat["nbr"].shape[1] == 1567027
     r = OracleSolver(lat, (0.52 - 0.5) / 3.0, model="regularised")
     workloads.configure(r, spec, lat, period=8000)
-    r.run(100)
+    r.run(STEPS)
     for order in ("c", "axis-split"):
         g = workloads.make_solver(spec, lat, period=8000, order=order)
-        g.run(100)
+        g.run(STEPS)
         compare(g, r)
 
 
