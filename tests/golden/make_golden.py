@@ -15,7 +15,9 @@ Outputs (in this folder):
   tables_hash.json   sha256 of phi / nbr / q / uin / coords plus link counts for full-size lattices
                      (validate.py's pipes and stenosis, the 24x24x64 periodic pipe, the R=24 open pipe);
   sponge.npz         tau per cell from `Solver.set_sponge` on a small open pipe;
-  units.json         `Units` conversions at the reference's operating points.
+  units.json         `Units` conversions at the reference's operating points;
+  circuit.json       the lumped circuit (simulate.circuit) and its calibration arithmetic (--circuit-only writes
+                     just this file).
 """
 import hashlib
 import json
@@ -275,5 +277,39 @@ def main(ref):
         print(f"  {k}: N={v['N']} counts={v['counts']}")
 
 
+def circuit(ref):
+    """circuit.json: the reference's lumped circuit (simulate.circuit, simulate.py:138-148) at three segment
+    resistances, and the calibrate branch's arithmetic (simulate.py:330-337) on two beat means, with the inputs
+    they read (vessel.py's flow targets and inflow waveform, simulate.py's outlet pressure)."""
+    _install_warp_stub()
+    sys.path.insert(0, ref)
+    import simulate
+    import vessel as V
+    _, shape = V.inflow_waveform(400)
+    out = {"inputs": {"q_in_ml_min": V.Q_INLET_MEAN, "q_target_ml_min": V.Q_MCA_TARGET,
+                      "p_out_mmhg": simulate.P_OUT_MMHG, "harmonics": simulate.HARMONICS,
+                      "shape": np.asarray(shape, float).tolist()},
+           "circuit": [], "recalibrate": []}
+    for R_seg in (0.0, 1.0e8, 3.0e9):
+        c = simulate.circuit(R_seg)
+        out["circuit"].append({"R_seg": R_seg, "R_out": [float(x) for x in c["R_out"]],
+                               "P_in_coef": [float(x) for x in c["P_in_coef"]], "R_eq": float(c["R_eq"])})
+    cal = simulate.circuit(0.0)
+    for p_in_mmhg, q_ml_min in ((92.0, 231.0), (101.5, 244.0)):
+        # the calibrate branch: R_tot from the beat's mean inlet pressure and inflow, then circuit(R_tot - R_eq)
+        p_in = p_in_mmhg * simulate.MMHG
+        R_tot = p_in / (q_ml_min * 1e-6 / 60)
+        c = simulate.circuit(float(max(R_tot - cal["R_eq"], 0.0)))
+        out["recalibrate"].append({"p_in_pa": p_in, "q_in_ml_min": q_ml_min, "R_seg": float(c["R_seg"]),
+                                   "P_in_coef": [float(x) for x in c["P_in_coef"]]})
+    with open(os.path.join(HERE, "circuit.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote circuit.json")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CEREBROSIM_REF", "."))
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    ref_dir = args[0] if args else os.environ.get("CEREBROSIM_REF", ".")
+    if "--circuit-only" not in sys.argv:
+        main(ref_dir)
+    circuit(ref_dir)

@@ -29,6 +29,26 @@ def test_circuit_and_recalibration():
     assert S.recalibrate(cal, 0.9 * p, 240.0, shape, 240.0, 135.0, 80.0)["R_seg"] == 0.0
 
 
+def test_circuit_matches_the_reference_golden():
+    """The circuit and the calibrate branch against the reference's own simulate.circuit (tests/golden/circuit.json,
+    written by make_golden.py from the reference's code and its flow targets and inflow waveform)."""
+    import json
+    import os
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "circuit.json")))
+    a = g["inputs"]
+    args = (np.asarray(a["shape"]), a["q_in_ml_min"], a["q_target_ml_min"], a["p_out_mmhg"])
+    for ref in g["circuit"]:
+        cal = S.circuit(ref["R_seg"], *args, nh=a["harmonics"])
+        np.testing.assert_allclose(cal["R_out"], ref["R_out"], rtol=1e-13)
+        np.testing.assert_allclose(cal["P_in_coef"], ref["P_in_coef"], rtol=1e-11, atol=1e-9)
+        assert cal["R_eq"] == pytest.approx(ref["R_eq"], rel=1e-13)
+    cal0 = S.circuit(0.0, *args, nh=a["harmonics"])
+    for ref in g["recalibrate"]:
+        cal = S.recalibrate(cal0, ref["p_in_pa"], ref["q_in_ml_min"], *args)
+        assert cal["R_seg"] == pytest.approx(ref["R_seg"], rel=1e-13)
+        np.testing.assert_allclose(cal["P_in_coef"], ref["P_in_coef"], rtol=1e-11, atol=1e-9)
+
+
 def test_coarse_bins():
     rng = np.random.default_rng(0)
     coords = np.unique(rng.integers(0, 20, size=(500, 3)), axis=0)
