@@ -47,7 +47,7 @@ class StepDesc(ctypes.Structure):
                 ("q_part", ctypes.c_void_p), ("fb_list", ctypes.c_void_p), ("n_fb", ctypes.c_int32),
                 ("q_last", ctypes.c_void_p), ("p_out64", ctypes.c_void_p),
                 ("r_out", ctypes.c_void_p), ("pref", ctypes.c_double), ("alpha", ctypes.c_double),
-                ("gblock", ctypes.c_int32 * 28)]
+                ("gblock", ctypes.c_int32 * 28), ("beat_acc", ctypes.c_void_p)]
 
 
 class BatchDesc(ctypes.Structure):

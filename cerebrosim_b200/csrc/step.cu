@@ -773,14 +773,21 @@ __device__ __forceinline__ void bc_body(const cs_step_desc& d) {
     if (k >= d.n_open) return;
     const double qk = s_q[k];
     d.q_last[k] = qk;
+    double pk;
     if (k == 0) {
         const float dv = *d.drive;
         d.p_out[0] = dv;
-        d.p_out64[0] = double(dv);
+        pk = double(dv);
     } else {
-        const double p = d.p_out64[k] + d.alpha * (double(d.r_out[k]) * qk - d.pref - d.p_out64[k]);
-        d.p_out64[k] = p;
-        d.p_out[k] = float(p);
+        pk = d.p_out64[k] + d.alpha * (double(d.r_out[k]) * qk - d.pref - d.p_out64[k]);
+        d.p_out[k] = float(pk);
+    }
+    d.p_out64[k] = pk;
+    if (d.beat_acc) {
+        // running sums for the beat means of the open ends' pressure and flow (one thread per open end)
+        d.beat_acc[k] += pk;
+        d.beat_acc[d.n_open + k] += qk;
+        if (k == 0) d.beat_acc[2 * d.n_open] += 1.0;
     }
 }
 

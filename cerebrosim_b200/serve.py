@@ -49,6 +49,7 @@ class Request:
         self.solver = None
         self.steps_total = 0
         self.steps_enq = 0
+        self.evicted = None          # beat after which the request was evicted for diverging
 
     @property
     def queue_wait(self):
@@ -80,7 +81,11 @@ class Server:
     launch shape and node order of every request's solver (autotune.tune picks them); schedule: the batch's schedule
     (batch.SCHEDULES; autotune.tune_schedule picks it); on_beat(request, beat): called
     when a request completes a beat (not its last), with its solver's state final for that beat — what it changes
-    (a recalibrated drive: simulate.recalibrate) applies from the next beat's first step."""
+    (a recalibrated drive: recalibrate_on_beat) applies from the next beat's first step.
+
+    Divergence: at every beat end (before on_beat) a request's densities are checked for non-finite values
+    (simulate.py:321-322 raises there); a request that has diverged is evicted at once — its steps stop, its slot and
+    budget are released, and it ends with ok = False and `evicted` = the beat — while the others go on unchanged."""
 
     def __init__(self, budget_bytes=150e9, storage="bf16", steps_per_beat=8000, chunk=1000, graph_chunk=200,
                  max_active=64, block=128, ahead=2, keep_fields=True, device=None, builder=default_builder,
@@ -130,18 +135,43 @@ class Server:
                 r.fields = s.fields()
         r.solver = None
 
+    def _finite(self, r):
+        """Densities all finite? Reduced on the side stream, which does not wait for the batch: chunks enqueued
+        after this beat may be running, and a value from any later step is as good (a non-finite density stays
+        non-finite)."""
+        with torch.cuda.stream(self._side):
+            return bool(torch.isfinite(r.solver.rho).all().item())
+
+    def _evict(self, r, beat, t):
+        """Stop a diverged request: leave the batch once the chunks already enqueued for it have run, release its
+        slot and budget."""
+        s = r.solver
+        if s in self._batch.members:
+            self._batch.remove(s, sync=True)
+        if r in self._active:
+            self._active.remove(r)
+        r.evicted, r.ok, r.done, r.solver = int(beat), False, t, None
+        return r.bytes_reserved
+
     def _complete(self, item, base, start):
-        """A chunk has completed: record beat ends, call on_beat, finish the requests it ended; returns the bytes
-        those requests release."""
+        """A chunk has completed: record beat ends, check for divergence, call on_beat, finish the requests it
+        ended; returns the bytes those requests release."""
         ev, snap = item
         ev.synchronize()
         t = base + start.elapsed_time(ev) / 1e3
         freed = 0.0
         for r, steps in snap:
+            if r.evicted is not None:
+                continue
             if steps % self.steps_per_beat == 0:
                 r.beat_end.append(t)
-                if self.on_beat is not None and steps < r.steps_total:
-                    self.on_beat(r, steps // self.steps_per_beat)
+                if steps < r.steps_total:
+                    beat = steps // self.steps_per_beat
+                    if not self._finite(r):
+                        freed += self._evict(r, beat, t)
+                        continue
+                    if self.on_beat is not None:
+                        self.on_beat(r, beat)
             if steps >= r.steps_total:
                 self._finish(r, t)
                 freed += r.bytes_reserved
@@ -165,6 +195,7 @@ class Server:
         inflight = collections.deque()     # (event, [(request, steps enqueued after this chunk)])
         self._used = 0.0
         batch = None
+        self._batch, self._active = None, active
         self._side = torch.cuda.Stream(self.device)
         t0 = time.perf_counter()
         start = None
@@ -183,7 +214,7 @@ class Server:
                     break
                 queue.popleft()
                 if batch is None:
-                    batch = BatchSolver(block=self.block, schedule=self.schedule)
+                    batch = self._batch = BatchSolver(block=self.block, schedule=self.schedule)
                 self._admit(r, batch, t0)
                 if start is None:
                     start = torch.cuda.Event(enable_timing=True)
@@ -198,7 +229,7 @@ class Server:
                 # a member has just been given its beat's last chunk: let it finish, so that on_beat sees the beat's
                 # final state and what it changes applies from the next beat's first step (simulate.py:330-337)
                 self._drain(inflight, base, start, active)
-            if active:
+            if active and batch.members:
                 batch.run(self.chunk, chunk=self.graph_chunk)
                 ev = torch.cuda.Event(enable_timing=True)
                 ev.record(batch.stream)
@@ -218,21 +249,29 @@ class Server:
             if not active and not inflight and not queue and pending and realtime:
                 time.sleep(max(0.0, min(0.05, pending[0].arrival - (time.perf_counter() - t0))))
         del batch
+        self._batch = self._active = None
         return reqs
+
+
+def recalibrate_on_beat(r, beat):
+    """Server on_beat hook for requests built by workloads.calibrated_builder: the lumped circuit recalibrated from
+    the beat's mean inlet pressure and inflow, its new inlet pressure driving the next beat (simulate.py:330-337)."""
+    r.solver.calibration.on_beat(beat)
 
 
 def summary(reqs, steps_per_beat):
     """p50 / p99 of the per-beat latency and of the queue wait, and aggregate MLUPS over the whole stream."""
     lat = np.array([x for r in reqs for x in r.beat_latencies()])
+    evicted = [r.id for r in reqs if r.evicted is not None]
     wait = np.array([r.queue_wait for r in reqs])
-    lu = sum(r.N * r.beats * steps_per_beat for r in reqs)
+    lu = sum(r.N * (r.beats if r.evicted is None else r.evicted) * steps_per_beat for r in reqs)
     t_first = min(r.arrival for r in reqs)
     t_last = max(r.done for r in reqs)
     return {"requests": len(reqs), "beats": int(lat.size), "lattice_updates": float(lu),
             "beat_latency_p50_s": float(np.percentile(lat, 50)), "beat_latency_p99_s": float(np.percentile(lat, 99)),
             "queue_wait_p50_s": float(np.percentile(wait, 50)), "queue_wait_p99_s": float(np.percentile(wait, 99)),
             "makespan_s": float(t_last - t_first), "mlups": float(lu / max(t_last - t_first, 1e-9) / 1e6),
-            "all_ok": bool(all(r.ok for r in reqs))}
+            "all_ok": bool(all(r.ok for r in reqs)), "evicted": evicted}
 
 
 def one_by_one(specs, storage="f32", steps_per_beat=8000, graph_chunk=200, block=None, device=None,

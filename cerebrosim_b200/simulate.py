@@ -80,6 +80,8 @@ class ArterySolver(Solver):
             self._qacc = torch.zeros(n_open, dtype=torch.float64, device=dev)
             self._qlast = torch.zeros(n_open, dtype=torch.float64, device=dev)
             self._r = torch.as_tensor(np.asarray(R_lu, np.float32)).to(dev)
+            # running sums of the open ends' pressure and flow over the current beat, and the step count
+            self._beat_acc = torch.zeros(2 * self.MAX_OPEN + 1, dtype=torch.float64, device=dev)
         self.pref = float(pref_lu)
         self.alpha = float(alpha)
         self.Qacc = DeviceArray(self._qacc, self.stream)
@@ -113,6 +115,21 @@ class ArterySolver(Solver):
         d.q_part, d.fb_list, d.n_fb = self._q_part.data_ptr(), self._fb_list.data_ptr(), self._n_fb
         d.q_last, d.r_out = self._qlast.data_ptr(), self._r.data_ptr()
         d.pref, d.alpha = self.pref, self.alpha
+        d.beat_acc = self._beat_acc.data_ptr()
+
+    def beat_means(self, reset=True):
+        """Means of the open ends' pressures p_out (lattice units) and flows Qlast over the steps since the last
+        reset, accumulated on the device in FP64 by every step's k_bc -> (p (n_open,), Q (n_open,), steps). The
+        reference averages its 1 ms samples of the same series over the beat (simulate.py:325-333)."""
+        self.stream.synchronize()
+        acc = self._beat_acc.cpu().numpy()
+        n = self.n_open
+        steps = int(round(acc[2 * n]))
+        if reset:
+            with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+                self._beat_acc.zero_()
+        k = max(steps, 1)
+        return acc[:n] / k, acc[n:2 * n] / k, steps
 
 
 # ---------------------------------------------------------------------------------------------------------------
@@ -281,6 +298,82 @@ def recalibrate(cal, p_in_mean_pa, q_in_mean_ml_min, shape, q_in_ml_min, q_targe
     inlet pressure and inflow, and the circuit rebuilt with it."""
     R_tot = p_in_mean_pa / (q_in_mean_ml_min * 1e-6 / 60)
     return circuit(max(R_tot - cal["R_eq"], 0.0), shape, q_in_ml_min, q_target_ml_min, p_out_mmhg)
+
+
+def flux_slabs(lat, ends, dx_mm, slab_mm=(2.5, 3.5), reach=1.3):
+    """simulate.py:181-192: the cells of each open end's flow slab — depth slab_mm inside the end (mm along the
+    inward normal), within `reach` radii of its axis — with weight sign * normal / thickness (inflow positive at end
+    0, outflow positive at the others) -> the ArterySolver's flux dict."""
+    P = np.asarray(lat["origin"], float) + np.asarray(lat["coords"], float) * dx_mm
+    thick = (slab_mm[1] - slab_mm[0]) / dx_mm
+    idx, w, slot = [], [], []
+    for k, e in enumerate(ends):
+        c, nrm = np.asarray(e["centre"], float), np.asarray(e["normal"], float)
+        rel = P - c
+        depth = -(rel @ nrm)
+        side = np.linalg.norm(rel + depth[:, None] * nrm, axis=1) < reach * e["radius"]
+        m = np.flatnonzero(side & (depth >= slab_mm[0]) & (depth < slab_mm[1]))
+        sign = -1.0 if k == 0 else 1.0
+        idx.append(m)
+        slot.append(np.full(len(m), k))
+        w.append(np.tile(sign * nrm / thick, (len(m), 1)))
+    return {"idx": np.concatenate(idx).astype(np.int32), "w": np.vstack(w).astype(np.float32),
+            "slot": np.concatenate(slot).astype(np.int32)}
+
+
+class Calibration:
+    """The inlet-pressure calibration of simulate.run (simulate.py:265-289, 325-337) over an ArterySolver whose open
+    end 0 is a pressure inlet (p_out[0] follows the drive) and whose other ends drain through resistances.
+
+    The lumped circuit (`circuit`) gives the outlet resistances and the inlet pressure waveform that draws the mean
+    inflow q_in (with the waveform `shape`, one period of samples with mean 1) through the segment resistance R_seg
+    plus the outlets. After each beat `on_beat` takes the beat's mean inlet pressure and inflow (the solver's
+    device-side beat means), finds the segment resistance they imply, rebuilds the circuit and sets the new drive,
+    which applies from the next beat's first step. SI units inside the circuit; the solver's lattice units through
+    `units` (lbm.Units) as q_si = dx^3 / dt and p_si = rho c^2."""
+
+    def __init__(self, units, shape, q_in_ml_min, q_target_ml_min, p_out_mmhg, steps_per_beat, ramp=0, flow=1.0,
+                 R_seg=0.0, nh=10):
+        self.un = units
+        self.shape = np.asarray(shape, float)
+        self.q_in, self.q_target, self.p_out_mmhg = float(q_in_ml_min), float(q_target_ml_min), float(p_out_mmhg)
+        self.spb, self.ramp, self.flow, self.nh = int(steps_per_beat), int(ramp), float(flow), int(nh)
+        self.q_si = units.dx ** 3 / units.dt
+        self.p_si = units.rho * units.c ** 2
+        self.pref_lu = self.p_out_mmhg * MMHG / self.p_si
+        self.cal = circuit(R_seg, self.shape, self.q_in, self.q_target, self.p_out_mmhg, nh)
+        self.history = []
+        self.s = None
+
+    def R_lu(self, n_open):
+        """Resistance per open end in lattice units (end 0, the inlet, has none)."""
+        return [r * self.q_si / self.p_si for r in self.cal["R_out"][:n_open]]
+
+    def attach(self, s):
+        """Set the solver's outlet pressures to the reference (gauge 0 at the inlet, -pref elsewhere) and its
+        drive from the current circuit."""
+        self.s = s
+        s.set_outlet_pressure([0.0] + [-self.pref_lu] * (s.n_open - 1))
+        self.drive()
+        s.beat_means(reset=True)
+        return s
+
+    def drive(self):
+        """simulate.py:284-289: the circuit's inlet pressure in lattice units, gauge, scaled by `flow`."""
+        c = np.array(self.cal["P_in_coef"]) / self.p_si * self.flow
+        c[0] -= self.pref_lu
+        self.s.set_drive(c, period=self.spb, ramp=self.ramp)
+
+    def on_beat(self, beat):
+        """simulate.py:325-337: the beat's mean inlet pressure (Pa, absolute) and inflow (mL/min) -> recalibrated
+        circuit -> the next beat's drive."""
+        p, q, steps = self.s.beat_means(reset=True)
+        p_in = float(self.un.p(p[0])) + self.p_out_mmhg * MMHG
+        q_in = float(q[0]) * self.q_si * 6e7
+        self.cal = recalibrate(self.cal, p_in, q_in, self.shape, self.q_in, self.q_target, self.p_out_mmhg)
+        self.history.append({"beat": int(beat), "steps": steps, "p_in_pa": p_in, "q_in_ml_min": q_in,
+                             "R_seg": self.cal["R_seg"]})
+        self.drive()
 
 
 def save(d, meta, series, frames, cmap=None, lat=None, wall_mm=None, dx_mm=None):

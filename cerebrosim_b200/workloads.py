@@ -212,3 +212,63 @@ def build_spec(spec, storage="f32", block=None, device=None, **kw):
     """Vessel, lattice and solver of a spec -> (solver, geometry, lattice, dx)."""
     g, lat, dx = spec_lattice(spec, device=device)
     return make_solver(spec, lat, storage=storage, block=block, device=device, **kw), g, lat, dx
+
+
+RHO = 1060.0             # kg/m^3, blood (the reference's vessel.py constants)
+NU = 3.5e-3 / RHO        # m^2/s
+
+
+def pressure_ends(g):
+    """The vessel's open ends as pressure boundaries (all of build_lattice's "outlet" kind), the feeding end first:
+    end 0 takes the drive as its pressure, the others drain through resistances (simulate.py's ends)."""
+    return [dict(o, kind="outlet") for o in openings(g)]
+
+
+def calibrated_solver(spec, dx_mm=None, storage="f32", block=None, device=None, order="c", steps_per_beat=8000,
+                      tau=0.52, pref_lu=0.004, target_share=135.0 / 240.0, relax_steps=100, sponge=(8, 0.6)):
+    """A generated vessel run as simulate.run runs the reference's arteries (simulate.py:253-337): pressure inlet
+    driven by the lumped circuit's inlet pressure, resistance outlets relaxed towards R Q - pref, flow measured on
+    slabs inside each end, and the inlet pressure recalibrated after every beat from the beat's mean inlet pressure
+    and inflow (`simulate.Calibration`, attached as `.calibration`).
+
+    Units: dx from the spec (its node count) unless given; dt such that tau holds for blood's viscosity. The target
+    mean inflow is the vessel's nominal mean inlet velocity (inflow_scale) through the inlet's area, target_share of
+    it for the parent's outlet (the reference's MCA share, 135 of 240 mL/min); the outlets' mean pressure pref_lu
+    (lattice units) sets the pressure scale; the inflow waveform is the vessel's seeded Fourier drive, normalised
+    to mean 1. The spec's vessel must not be occluded (the parent must carry the flow from end 0)."""
+    from . import simulate as S
+    g = stenosed_vessel(seed=spec["seed"], stenosis=spec["stenosis"])
+    if g["occluded"]:
+        raise ValueError("a calibrated vessel needs an open parent")
+    dx_mm = dx_mm or spec.get("dx") or dx_for_nodes(spec["nodes"], estimated_nodes(g, 0.05), 0.05)
+    ends = pressure_ends(g)
+    lat = vessel.artery_lattice(g, dx_mm, openings=ends, device=device)
+    nu_lu = (tau - 0.5) / 3.0
+    dx = dx_mm * 1e-3
+    un = lbm.Units(dx, nu_lu * dx * dx / NU, RHO, NU)
+    u_lu = inflow_scale(spec["pressure"], spec["stenosis"])
+    q_in = u_lu * un.c * math.pi * (ends[0]["radius"] * 1e-3) ** 2 * 6e7          # mL/min
+    coef = fourier_drive(spec["seed"])
+    t = np.arange(400) / 400.0
+    wave = coef[0] + sum(coef[2 * k - 1] * np.cos(2 * np.pi * k * t) + coef[2 * k] * np.sin(2 * np.pi * k * t)
+                         for k in range(1, (len(coef) - 1) // 2 + 1))
+    p_out_mmhg = pref_lu * RHO * un.c ** 2 / S.MMHG
+    cal = S.Calibration(un, wave / wave.mean(), q_in, target_share * q_in, p_out_mmhg, steps_per_beat,
+                        ramp=min(1000, steps_per_beat // 8))
+    flux = S.flux_slabs(lat, ends, dx_mm)
+    s = S.ArterySolver(lat, nu_lu, flux, cal.R_lu(len(ends)), cal.pref_lu, 1.0 / relax_steps, model="regularised",
+                       storage=storage, block=block, device=device, order=order)
+    s.set_sponge(sponge[0], sponge[1], kinds=("outlet",))
+    cal.attach(s)
+    s.calibration = cal
+    return s
+
+
+def calibrated_builder(spec, storage, block, device, steps_per_beat, order="c"):
+    """serve.Server builder of calibrated requests (pair with serve.recalibrate_on_beat)."""
+    s = calibrated_solver(spec, storage=storage, block=block, device=device, order=order,
+                          steps_per_beat=steps_per_beat)
+    for k in ("nbr", "q", "_dev"):
+        s.lat.pop(k, None)
+    return s
+

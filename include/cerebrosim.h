@@ -209,6 +209,10 @@ typedef struct cs_step_desc {
      * gblock[27] = the number of 256-slot blocks over all directions). All zero: the padded grid, ceil(gmax / 256)
      * blocks for every direction. */
     int32_t gblock[28];
+    /* Beat means of the resistance coupling (n_open > 0; null: none): k_bc adds, every step, p_out64[k] to
+     * beat_acc[k] and q_last[k] to beat_acc[n_open + k] (FP64) and 1 to beat_acc[2 * n_open]; the caller zeroes
+     * it at a beat's start and divides by the count at its end (the beat means of simulate.py:325-333). */
+    double* beat_acc;
 } cs_step_desc;
 
 /* Block partition of a sorted flux list for `block` threads per block: out[b] = first entry with

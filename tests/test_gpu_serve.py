@@ -97,3 +97,68 @@ def test_on_beat_changes_apply_from_the_next_beat():
         s.run(SPB, chunk=50)
         p, u = s.fields()
         assert l2(r.fields[1], u) <= 1e-5, r.id
+
+
+def test_diverged_request_is_evicted_and_the_others_are_unchanged():
+    """One request's populations are poisoned with NaN from the host after its first beat (a density that has gone
+    non-finite, as a diverging run's does). At its next beat end the server evicts it — slot and budget released —
+    while every other request ends bit for bit where it ends when served alone."""
+    import torch
+    poisoned = 2                                     # three beats
+
+    def poison(r, beat):
+        if r.id == poisoned and beat == 1:
+            s = r.solver
+            with torch.cuda.stream(s.stream):
+                s.f[s.cur][0, 10] = float("nan")
+            s.synchronize()
+
+    sv = server("f32", max_active=3, on_beat=poison)
+    mix = sv.serve(specs(), realtime=False)
+    bad = next(r for r in mix if r.id == poisoned)
+    assert bad.evicted == 2 and bad.ok is False and bad.fields is None and bad.solver is None
+    assert len(bad.beat_end) == 2
+    st = serve.summary(mix, SPB)
+    assert st["evicted"] == [poisoned] and not st["all_ok"]
+    assert sv._used == pytest.approx(0.0, abs=1.0)   # every reservation released, the evicted one included
+    for r in mix:
+        if r.id == poisoned:
+            continue
+        assert r.ok and r.evicted is None
+        alone = server("f32").serve([r.spec], realtime=False)[0]
+        assert np.array_equal(alone.fields[0], r.fields[0]) and np.array_equal(alone.fields[1], r.fields[1]), r.id
+
+
+def calibrated_specs():
+    return [{"id": k, "arrival": 0.0, "seed": 300 + k, "stenosis": s, "pressure": p, "beats": 3, "nodes": n}
+            for k, (s, p, n) in enumerate([(0.5, 90.0, 30e3), (0.0, 120.0, 45e3), (0.7, 75.0, 25e3)])]
+
+
+def test_served_recalibration_matches_dedicated_artery_solver():
+    """Requests run as the reference runs its arteries (pressure inlet from the lumped circuit, resistance outlets,
+    slab flows) with the circuit recalibrated after every beat from the beat's mean inlet pressure and inflow
+    (simulate.py:330-337), served three at a time: each ends as the same schedule on a dedicated ArterySolver, with
+    the same segment resistance found at every beat."""
+    seen = {}
+
+    def hook(r, beat):
+        serve.recalibrate_on_beat(r, beat)
+        seen[(r.id, beat)] = dict(r.solver.calibration.history[-1])
+
+    sv = server("f32", max_active=3, builder=workloads.calibrated_builder, on_beat=hook)
+    mix = sv.serve(calibrated_specs(), realtime=False)
+    assert all(r.ok for r in mix)
+    for r in mix:
+        s = workloads.calibrated_solver(r.spec, storage="f32", block=128, steps_per_beat=SPB)
+        for b in range(1, r.beats + 1):
+            s.run(SPB, chunk=50)
+            if b < r.beats:
+                s.calibration.on_beat(b)
+                h, hs = s.calibration.history[-1], seen[(r.id, b)]
+                assert h["steps"] == hs["steps"] == SPB
+                assert h["R_seg"] == pytest.approx(hs["R_seg"], rel=1e-6, abs=1.0)
+                assert h["q_in_ml_min"] == pytest.approx(hs["q_in_ml_min"], rel=1e-6)
+        p, u = s.fields()
+        assert l2(r.fields[1], u) <= 1e-5 and l2(3 * r.fields[0] + 1, 3 * p + 1) <= 1e-5, r.id
+        # the calibration acted: a segment resistance was found from the measured beat means
+        assert any(seen[(r.id, b)]["R_seg"] > 0 for b in range(1, r.beats))
