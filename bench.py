@@ -118,22 +118,20 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(lat, max_seconds=20.0):
-    """The CPU restatement (FP32, OpenMP on every core) on a bounded number of full steps of the same lattice."""
-    from oracle.step_ref import OracleSolver
-    s = OracleSolver(lat, nu_lu(), model="regularised")
-    configure(s)
-    t = time.perf_counter()
-    s.run(2)
-    per = (time.perf_counter() - t) / 2
-    n = int(max(2, min(200, max_seconds / max(per, 1e-6))))
-    t = time.perf_counter()
-    s.run(n)
-    secs = time.perf_counter() - t
-    N = lat["nbr"].shape[1]
-    return {"value": N * n / secs / 1e6, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{n} full steps of the {N}-node lattice (FP32 CPU restatement of the reference step, "
-                      f"OpenMP, {os.cpu_count()} threads)"}
+def cpu_baseline_process(steps=400, warmup=20):
+    """The CPU baseline measured as the reference arm measures it — `bench.py --impl reference` in a process of its
+    own (the FP32 CPU restatement of the reference step, OpenMP on every host core) — started before this process
+    touches the GPU, so that nothing else competes for the host cores."""
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE")}
+    try:
+        out = subprocess.run([sys.executable, os.path.abspath(__file__), "--impl", "reference", "--steps", str(steps),
+                              "--warmup", str(warmup)], capture_output=True, text=True, env=env, timeout=600)
+        line = json.loads(out.stdout.strip().splitlines()[-1])
+    except (subprocess.SubprocessError, ValueError, IndexError) as e:
+        return {"error": f"CPU baseline process failed: {e}"}
+    cb = dict(line["cpu_baseline"])
+    cb["sample"] += "; measured in its own process before any GPU work (the reference arm's code and threads)"
+    return cb
 
 
 def run_reference(args):
@@ -163,6 +161,93 @@ def run_reference(args):
                                        f"reference step, FP32, OpenMP, {cores} threads)"},
             "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def artery_line(storage, steps, warmup, dev, peak, flush):
+    """The single-vessel configuration at full size: the generated stenosed artery of seed 3 at 0.05 mm (1,567,027
+    nodes), one solver, `steps` steps timed one by one with the L2 flushed before each (as the headline), and the
+    same steps back to back."""
+    import ctypes
+
+    import torch
+
+    from cerebrosim_b200 import _lib
+    lib = _lib.load()
+    s = case_solver("artery:3", storage, device=dev)
+    descs = [s._desc(), s._desc()]
+    sp = ctypes.c_void_p(s.stream.cuda_stream)
+
+    def step():
+        _lib.check(lib.cs_step(ctypes.byref(descs[s.cur]), s.cur, 1, sp))
+        s.cur = 1 - s.cur
+        s.steps += 1
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    with torch.cuda.stream(s.stream):
+        for k in range(warmup):
+            flush(k)
+            step()
+        for k in range(steps):
+            flush(k)
+            ev[k][0].record(s.stream)
+            step()
+            ev[k][1].record(s.stream)
+        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b0.record(s.stream)
+        _lib.check(lib.cs_step(ctypes.byref(descs[s.cur]), s.cur, steps, sp))
+        b1.record(s.stream)
+        s.stream.synchronize()
+    if steps % 2:
+        s.cur = 1 - s.cur
+    s.steps += steps
+    secs = sum(a.elapsed_time(b) for a, b in ev) * 1e-3
+    b2b = b0.elapsed_time(b1) * 1e-3
+    mlups = s.N * steps / secs / 1e6
+    bplu = BPLU[storage]
+    out = {"workload": "generated stenosed artery, seed 3, 0.05 mm (70 % cosine stenosis, 40 degree side branch, "
+                       "Fourier velocity inlet, two pressure outlets, sponge; tau 0.52)",
+           "nodes": s.N, "storage": storage, "block": s.block, "steps": steps, "value": mlups, "unit": "MLUPS",
+           "ms_per_step": secs / steps * 1e3, "hbm_gbs": bplu * mlups / 1e3, "frac": bplu * mlups / 1e3 / peak,
+           "bytes_per_update": bplu, "l2": "flushed between timed steps, as the headline",
+           "back_to_back": {"ms_per_step": b2b / steps * 1e3, "value": s.N * steps / b2b / 1e6, "unit": "MLUPS"},
+           "ok": s.ok()}
+    del s
+    return out
+
+
+def case_solver(name, storage, block=None, device=None):
+    """Solver of a named case: the pulsatile-pipe set-up for open pipes (plug inlet, its drive, pressure outlet,
+    tau 0.55), a body force for periodic pipes, or artery:SEED — the generated stenosed artery of that seed at
+    0.05 mm (70 % stenosis, side branch, Fourier inflow, tau 0.52)."""
+    from cerebrosim_b200 import cases, lbm, workloads
+    if name.startswith("artery:"):
+        seed = int(name.split(":")[1])
+        spec = {"seed": seed, "stenosis": 0.7, "pressure": 95.0}
+        lat = workloads.lattice(workloads.stenosed_vessel(seed), 0.05, device=device)
+        return workloads.make_solver(spec, lat, storage=storage, block=block, device=device)
+    lat = lbm.build_lattice(**cases.lattice_args(cases.case(name)), device=device)
+    if lat["n_outlets"] or any(o["kind"] == "inlet" for o in lat["openings"]):
+        s = lbm.Solver(cases.plug_inlet(lat), nu_lu(), model="regularised", storage=storage, block=block, device=device)
+        configure(s)
+    else:
+        s = lbm.Solver(lat, nu_lu(), model="regularised", storage=storage, block=block, device=device)
+        s.set_force([0.0, 0.0, 1e-6])
+    return s
+
+
+def run_profile(args):
+    """--profile CASE: warm-up and timed steps of one case (CUDA graphs of 100 steps), one JSON line."""
+    import torch
+    s = case_solver(args.profile, args.storage)
+    s.run(args.warmup, chunk=100)
+    s.synchronize()
+    t = time.perf_counter()
+    s.run(args.steps, chunk=100)
+    s.synchronize()
+    secs = time.perf_counter() - t
+    print(json.dumps({"case": args.profile, "nodes": s.N, "steps": args.steps, "storage": args.storage,
+                      "block": s.block, "mlups": s.N * args.steps / secs / 1e6, "ok": s.ok(),
+                      "gpu": torch.cuda.get_device_name()}), flush=True)
 
 
 def bench_sweep(args, dev, peak):
@@ -275,10 +360,21 @@ def main():
     ap.add_argument("--sweep-steps", type=int, default=8000, help="steps of the batched sweep (0: skip it)")
     ap.add_argument("--sweep-storage", default="f16", choices=["f32", "f16", "bf16"])
     ap.add_argument("--serve-requests", type=int, default=12, help="requests of the served stream (0: skip it)")
+    ap.add_argument("--artery-steps", type=int, default=None,
+                    help="timed steps of the 1.57 M-node artery lines (default: --steps, at most 400; 0: skip them)")
+    ap.add_argument("--profile", default=None, metavar="CASE",
+                    help="run only CASE (a named lattice of cerebrosim_b200.cases, or artery:SEED for the generated "
+                         "stenosed artery at 0.05 mm) for --warmup + --steps steps and print its throughput: the "
+                         "command the ncu summaries are captured from")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile:
+        return run_profile(args)
+    cpu_line = None
+    if int(os.environ.get("WORLD_SIZE", "1")) == 1 and not args.no_cpu_baseline:
+        cpu_line = cpu_baseline_process()
 
     import ctypes
 
@@ -412,20 +508,24 @@ def main():
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_kind": peak_kind,
                              "traffic": tr * N if tr else None, "bytes_per_update": bplu,
-                             "kernel": "one step = k_boundary + k_bulk_dense (timed together)"},
+                             "kernel": "one step = k_boundary + the bulk kernel (k_bulk_pair: two nodes per "
+                                       "thread), timed together"},
                 "back_to_back": {"ms_per_step": b2b * 1e3, "value": world * N / b2b / 1e6, "unit": "MLUPS",
                                  "note": "the same steps in one call without flushing: steady state with L2 reuse"},
                 "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "ok": ok,
                 "whole_region_ms": whole0.elapsed_time(whole1)}
         if clk:
             line["clocks"] = clk
+        a_steps = min(args.steps, 400) if args.artery_steps is None else args.artery_steps
+        if world == 1 and a_steps > 0:
+            line["artery"] = {st: artery_line(st, a_steps, min(args.warmup, 50), dev, peak, flush)
+                              for st in ("f32", "f16")}
         if world == 1 and args.sweep_steps > 0:
             line["batched"] = bench_sweep(args, dev, peak)
         if world == 1 and args.serve_requests > 0:
             line["served"] = bench_served(args, dev)
-        if world == 1 and not args.no_cpu_baseline:
-            from oracle import lattice_ref as L
-            line["cpu_baseline"] = cpu_baseline(cases.plug_inlet(L.build_lattice(**cases.lattice_args(c))))
+        if cpu_line is not None:
+            line["cpu_baseline"] = cpu_line
         print(json.dumps(line), flush=True)
     rep.close()
 

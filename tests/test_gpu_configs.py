@@ -93,7 +93,7 @@ def test_config2_womersley_four_periods():
     assert mid.sum() > 1500
     ax = np.asarray(c["meta"]["axis"], float)
     num = den = 0.0
-    flux = []
+    flux, inflow = [], []
     for _ in range(12):
         s.run(T // 12, chunk=1000)
         _, u = s.fields()
@@ -103,13 +103,17 @@ def test_config2_womersley_four_periods():
         exact = 2 * U0 * (1 - (rc[mid] / R) ** 2) + V.womersley_flow(rc[mid], R, Wo, -0.5j * U0, w, t)
         num += ((ua - exact) ** 2).sum()
         den += (exact ** 2).sum()
-        flux.append(ua.mean() / (U0 * (1 + 0.5 * math.sin(w * t))) - 1)
+        flux.append(ua.mean())
+        inflow.append(U0 * (1 + 0.5 * math.sin(w * t)))
     assert s.ok()
     e = math.sqrt(num / den)
-    print(f"config 2: Wo {Wo:.3f}, mid-section L2 over the fifth period {e:.4f}, cross-section mean vs inlet "
-          f"{min(flux):+.4f} .. {max(flux):+.4f}")
+    # over a period the mid-section carries the inflow (mass conservation); within a period the weakly compressible
+    # fluid delays it by the sound crossing time (about 170 steps to mid-length, a phase lag of 0.27 rad)
+    balance = sum(flux) / sum(inflow) - 1
+    print(f"config 2: Wo {Wo:.3f}, mid-section L2 over the fifth period {e:.4f}, period-mean flow at mid-length vs "
+          f"inlet {balance:+.4f}")
     assert e <= CFG2_BOUND
-    assert max(abs(x) for x in flux) <= 2e-2      # the inflow reaches mid-length (mass conservation)
+    assert abs(balance) <= 1e-2
 
 
 @pytest.fixture(scope="module")
