@@ -297,8 +297,9 @@ def bench_sweep(args, dev, peak):
     TUNED.update(schedule=sched["schedule"])
     out["autotune"]["schedule"] = {"best": sched["schedule"], "candidates": sched_table}
     b.run(400, chunk=200)
+    b.prepare(steps)                  # one CUDA graph per heartbeat and member (the fused schedule: per 400 steps)
     clocks = Clocks(dev.index)
-    secs = timed(lambda: b.run(steps, chunk=200))
+    secs = timed(lambda: b.run(steps, chunk=steps))
     out["clocks"] = clocks.stop()
     ok = all(x.ok() for x in sol)
     mlups = nodes * steps / secs / 1e6
@@ -306,8 +307,9 @@ def bench_sweep(args, dev, peak):
     out.update({"nodes": nodes, "storage": args.sweep_storage, "value": mlups, "unit": "MLUPS",
                 "hbm_gbs": bplu * mlups / 1e3, "frac": bplu * mlups / 1e3 / peak, "ok": ok,
                 "schedule": b.schedule, "seconds": secs,
-                # boundary + bulk per step: once per launch group of 64 (fused), once per member (by-instance)
-                "gpu_launches": 2 * steps * (len(sol) if b.schedule == "by-instance" else -(-len(sol) // 64))})
+                # boundary + bulk per step: once per launch group of 64 (fused), once per member (otherwise)
+                "gpu_launches": 2 * steps * (-(-len(sol) // 64) if b.schedule == "fused" else len(sol)),
+                "graph_steps": steps if b.schedule != "fused" else 400})
     del b, sol
     # the plain form: each vessel on its own dedicated FP32 solver, one after another
     tot = 0.0
@@ -315,7 +317,8 @@ def bench_sweep(args, dev, peak):
     for sp, lat in zip(specs, lats):
         x = W.make_solver(sp, lat, storage="f32", device=dev)
         x.run(400, chunk=200)
-        tot += timed(lambda: x.run(steps, chunk=200))
+        x.prepare(steps)
+        tot += timed(lambda: x.run(steps, chunk=steps))
         ok &= x.ok()
         del x
     plain = nodes * steps / tot / 1e6

@@ -16,8 +16,11 @@ buffers either way):
 - "fused": every step is one batched launch per kernel over all members (above);
 - "by-instance": each member advances a whole `run` with its own single-lattice kernels and graphs, one member after
   the other on the batch stream. A member whose working set fits in the L2 then keeps it there from step to step,
-  where the fused launches stream every member's populations through the L2 at every step; on a sweep of 0.3-3 M-node
-  vessels in FP16 this schedule is the faster one. `autotune` chooses between them by measurement.
+  where the fused launches stream every member's populations through the L2 at every step;
+- "concurrent:K": the members split into K groups of about equal node counts, each group by instance on a stream of
+  its own, the K streams at once: a small member's kernels (a grid of a wave or two) then share the GPU with another
+  group's instead of leaving SMs idle at every step's tail.
+`autotune.tune_schedule` chooses among them by measurement.
 """
 import ctypes
 
@@ -28,7 +31,10 @@ from ._lib import check
 from .lbm import ctypes_void
 
 MAX_GROUPS = 64          # launch groups of CS_BATCH_GROUP instances: up to 4096 instances per batch
-SCHEDULES = ("fused", "by-instance")
+# steps per CUDA graph of the fused schedule at most: each of its launches carries its group's 22 KB descriptor
+# table as kernel parameters, so a graph holds ~66 KB of parameters per step and group
+FUSED_GRAPH_MAX = 400
+SCHEDULES = ("fused", "by-instance", "concurrent:2", "concurrent:4")
 
 
 class BatchSolver:
@@ -39,7 +45,7 @@ class BatchSolver:
     per work item. schedule: "fused" or "by-instance" (module docstring)."""
 
     def __init__(self, solvers=(), block=128, persistent=True, device=None, schedule="fused"):
-        if schedule not in SCHEDULES:
+        if schedule not in SCHEDULES and not schedule.startswith("concurrent:"):
             raise ValueError(f"schedule {schedule!r}: one of {SCHEDULES}")
         self.members = []
         self.block = int(block)
@@ -141,15 +147,40 @@ class BatchSolver:
         for m in self.members:
             m.stream.wait_stream(self.stream)
 
+    def prepare(self, chunk):
+        """Capture the CUDA graphs a later `run(k * chunk, chunk=chunk)` replays (a whole heartbeat per graph, for
+        instance), so that the capture happens before a timed region rather than inside it."""
+        chunk += chunk % 2
+        if not self.members:
+            return
+        if self.schedule == "fused":
+            chunk = min(chunk, FUSED_GRAPH_MAX)
+            self._refresh()
+            key = (self.cur, chunk)
+            if key not in self.graphs:
+                lib = _lib.load()
+                g = ctypes.c_void_p()
+                self._sync_in()
+                with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+                    check(lib.cs_batch_graph_capture(ctypes.byref(self.desc), self.cur, chunk,
+                                                     ctypes_void(self.stream.cuda_stream), ctypes.byref(g)))
+                self.graphs[key] = g
+        else:
+            for m in self.members:
+                m.prepare(chunk)
+
     def run(self, steps, chunk=200):
         """Advance every member `steps` steps (CUDA graphs of `chunk` batched steps; chunk even)."""
         if not self.members:
             return
         if self.schedule == "by-instance":
             return self._run_by_instance(steps, chunk)
+        if self.schedule.startswith("concurrent"):
+            return self._run_concurrent(steps, chunk, int(self.schedule.split(":")[1]))
         self._refresh()
         lib = _lib.load()
         chunk += chunk % 2
+        chunk = min(chunk, FUSED_GRAPH_MAX)
         full, rest = divmod(int(steps), chunk)
         self._sync_in()
         sp = ctypes_void(self.stream.cuda_stream)
@@ -179,6 +210,31 @@ class BatchSolver:
         with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
             for m in self.members:
                 m.run(steps, chunk=chunk)          # advances m.cur and m.steps itself
+        self._sync_out()
+        self.steps += int(steps)
+        if int(steps) % 2:
+            self.cur = 1 - self.cur
+
+    def _run_concurrent(self, steps, chunk, k):
+        """Groups of members of about equal node counts (largest first into the lightest group), each group by
+        instance on its own stream, the streams concurrently; the batch stream then waits for all of them."""
+        k = max(1, min(k, len(self.members)))
+        if len(getattr(self, "_streams", [])) < k:
+            self._streams = [torch.cuda.Stream(self.dev) for _ in range(k)]
+        groups, load = [[] for _ in range(k)], [0] * k
+        for m in sorted(self.members, key=lambda m: -m.N):
+            j = load.index(min(load))
+            groups[j].append(m)
+            load[j] += m.N
+        self._sync_in()
+        with torch.cuda.device(self.dev):
+            for st, grp in zip(self._streams, groups):
+                st.wait_stream(self.stream)
+                with torch.cuda.stream(st):
+                    for m in grp:
+                        m.run(steps, chunk=chunk)
+            for st in self._streams[:k]:
+                self.stream.wait_stream(st)
         self._sync_out()
         self.steps += int(steps)
         if int(steps) % 2:

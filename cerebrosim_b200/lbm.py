@@ -387,6 +387,16 @@ class Solver:
         else:
             check(_lib.load().cs_graph_launch(g, ctypes_void(self.stream.cuda_stream)))
 
+    def prepare(self, chunk):
+        """Capture the CUDA graph of `chunk` steps that the next `run(k * chunk, chunk=chunk)` replays (for a graph
+        of a whole heartbeat, captured before a timed run); nothing is launched."""
+        chunk += chunk % 2
+        key = (self.cur, chunk)
+        if key not in self.graphs:
+            self.stream.wait_stream(torch.cuda.current_stream(self.dev))
+            with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+                self.graphs[key] = self._capture(self.cur, chunk)
+
     def run(self, steps, chunk=200):
         """Advance `steps` steps (CUDA graphs of `chunk` steps; chunk even), lbm.py:430-448."""
         chunk += chunk % 2

@@ -134,11 +134,14 @@ def test_batch_members_join_and_leave(golden):
         same(a, m)
 
 
-def test_by_instance_schedule_is_the_solo_run(golden):
+@pytest.mark.parametrize("schedule", ["by-instance", "concurrent:2", "concurrent:4"])
+def test_by_instance_schedule_is_the_solo_run(golden, schedule):
+    """Member after member on the batch stream, or in groups on concurrent streams: each member's run is its solo
+    run, bit for bit, joins and leaves included."""
     solo = [make(golden, n, c, k) for n, c, k in SPECS]
     mixed = [make(golden, n, c, k) for n, c, k in SPECS]
     fused = [make(golden, n, c, k) for n, c, k in SPECS]
-    b = BatchSolver(mixed[:3], schedule="by-instance")
+    b = BatchSolver(mixed[:3], schedule=schedule)
     b.run(101, chunk=40)
     b.remove(mixed[1])
     b.add(mixed[3])
@@ -160,7 +163,7 @@ def test_by_instance_schedule_is_the_solo_run(golden):
         close(a, m)
 
 
-def test_schedule_tuning_times_both_and_keeps_the_faster(golden):
+def test_schedule_tuning_times_each_and_keeps_the_fastest(golden):
     from cerebrosim_b200 import autotune
     from cerebrosim_b200.batch import SCHEDULES
     members = [make(golden, n, c, k) for n, c, k in SPECS[:2]]
@@ -169,7 +172,8 @@ def test_schedule_tuning_times_both_and_keeps_the_faster(golden):
     assert [r["schedule"] for r in table] == list(SCHEDULES)
     assert best["schedule"] == b.schedule == min(table, key=lambda r: r["us_per_step"])["schedule"]
     assert all(r["us_per_step"] > 0 for r in table)
-    assert b.steps == 60 and all(m.steps == 60 and m.ok() for m in members)
+    k = 30 * len(SCHEDULES)
+    assert b.steps == k and all(m.steps == k and m.ok() for m in members)
 
 
 def test_coupled_runs_are_reproducible(golden):
