@@ -250,9 +250,11 @@ def run_profile(args):
                       "gpu": torch.cuda.get_device_name()}), flush=True)
 
 
-def bench_sweep(args, dev, peak):
+def bench_sweep(args, dev, peak, rep):
     """The batched sweep: 16 generated vessels (seeds 100-115, stenosis 0-100 %, 70-145 mmHg, 0.3-3 M nodes) in
-    one batched launch per kernel and step, 16-bit storage, against the plain form (each vessel alone, FP32)."""
+    one batch, 16-bit storage, against the plain form (each vessel alone, FP32). With several ranks each rank runs
+    its round-robin share of the vessels (Replicas.share) and the rates are the whole job's: all ranks' node
+    updates over the slowest rank's time."""
     import torch
 
     from cerebrosim_b200 import workloads as W
@@ -260,7 +262,7 @@ def bench_sweep(args, dev, peak):
 
     from cerebrosim_b200 import autotune
 
-    specs = W.sweep()
+    specs = rep.share(W.sweep())
     t0 = time.perf_counter()
     lats = [W.spec_lattice(sp, device=dev)[1] for sp in specs]
     build_s = time.perf_counter() - t0
@@ -302,10 +304,11 @@ def bench_sweep(args, dev, peak):
     secs = timed(lambda: b.run(steps, chunk=steps))
     out["clocks"] = clocks.stop()
     ok = all(x.ok() for x in sol)
-    mlups = nodes * steps / secs / 1e6
+    mlups = rep.rate(nodes * steps, secs) / 1e6
     bplu = BPLU[args.sweep_storage]
-    out.update({"nodes": nodes, "storage": args.sweep_storage, "value": mlups, "unit": "MLUPS",
-                "hbm_gbs": bplu * mlups / 1e3, "frac": bplu * mlups / 1e3 / peak, "ok": ok,
+    out.update({"nodes": int(rep.sum(nodes)), "instances": int(rep.sum(len(specs))), "ranks": rep.world,
+                "storage": args.sweep_storage, "value": mlups, "unit": "MLUPS",
+                "hbm_gbs": bplu * mlups / 1e3, "frac": bplu * mlups / 1e3 / (peak * rep.world), "ok": ok,
                 "schedule": b.schedule, "seconds": secs,
                 # boundary + bulk per step: once per launch group of 64 (fused), once per member (otherwise)
                 "gpu_launches": 2 * steps * (-(-len(sol) // 64) if b.schedule == "fused" else len(sol)),
@@ -321,19 +324,19 @@ def bench_sweep(args, dev, peak):
         tot += timed(lambda: x.run(steps, chunk=steps))
         ok &= x.ok()
         del x
-    plain = nodes * steps / tot / 1e6
+    plain = rep.rate(nodes * steps, tot) / 1e6
     out["plain_f32_one_by_one"] = {"value": plain, "unit": "MLUPS", "hbm_gbs": BPLU["f32"] * plain / 1e3,
-                                   "frac": BPLU["f32"] * plain / 1e3 / peak, "ok": ok, "seconds": tot}
+                                   "frac": BPLU["f32"] * plain / 1e3 / (peak * rep.world), "ok": ok, "seconds": tot}
     out["speedup_vs_plain"] = mlups / plain
     return out
 
 
-def bench_served(args, dev):
+def bench_served(args, dev, rep):
     """The served stream: Poisson arrivals (2/s, seed 5), clot U[0, 100] %, pressure U[70, 145] mmHg, 1-4 beats of
     8000 steps, 0.2-4 M nodes, 150 GB budget, 16-bit storage; against the same requests one by one in plain FP32."""
     from cerebrosim_b200 import serve, workloads as W
 
-    specs = W.request_stream(args.serve_requests, seed=5)
+    specs = rep.share(W.request_stream(args.serve_requests, seed=5))
     sv = serve.Server(budget_bytes=150e9, storage=args.sweep_storage, steps_per_beat=8000, chunk=1000,
                       graph_chunk=200, device=dev, keep_fields=True, block=TUNED["block"], order=TUNED["order"],
                       schedule=TUNED["schedule"])
@@ -342,11 +345,21 @@ def bench_served(args, dev):
     clk = clocks.stop()
     st = serve.summary(reqs, 8000)
     st["clocks"] = clk
+    if rep.world > 1:
+        # the whole job: every rank's beats for the percentiles, all updates over the slowest rank's makespan
+        lat = [x for part in rep.gather([x for r in reqs for x in r.beat_latencies()]) for x in part]
+        wait = [x for part in rep.gather([r.queue_wait for r in reqs]) for x in part]
+        st.update({"beat_latency_p50_s": float(np.percentile(lat, 50)), "beat_latency_p99_s": float(np.percentile(lat, 99)),
+                   "queue_wait_p50_s": float(np.percentile(wait, 50)), "queue_wait_p99_s": float(np.percentile(wait, 99)),
+                   "mlups": rep.rate(st["lattice_updates"], st["makespan_s"]) / 1e6, "ranks": rep.world,
+                   "requests": int(rep.sum(len(reqs)))})
     st.update({"workload": f"first {len(specs)} requests of the seed-5 Poisson stream (2 requests/s)",
                "storage": args.sweep_storage, "budget_gb": 150.0, "block": TUNED["block"], "order": TUNED["order"], "schedule": TUNED["schedule"],
                "max_active": max(n for _, n, _ in sv.trace),
                "peak_reserved_gb": max(u for _, _, u in sv.trace) / 1e9})
     plain = serve.one_by_one(specs, storage="f32", steps_per_beat=8000, device=dev)
+    if rep.world > 1:
+        plain["mlups"] = rep.rate(plain["lattice_updates"], plain["seconds"]) / 1e6
     st["plain_f32_one_by_one"] = plain
     st["speedup_vs_plain"] = st["mlups"] / plain["mlups"]
     return st
@@ -495,6 +508,13 @@ def main():
            "definition": "Solver(lat) from pinned host tables + run(K) in CUDA graphs + fields() readback, "
                          "no L2 flush"}
 
+    # the batched sweep and the served stream: every rank runs its share (the same collective calls on every rank)
+    extra = {}
+    if args.sweep_steps > 0:
+        extra["batched"] = bench_sweep(args, dev, peak, rep)
+    if args.serve_requests > 0:
+        extra["served"] = bench_served(args, dev, rep)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": mean_step * 1e3, "higher_is_better": True,
@@ -523,10 +543,7 @@ def main():
         if world == 1 and a_steps > 0:
             line["artery"] = {st: artery_line(st, a_steps, min(args.warmup, 50), dev, peak, flush)
                               for st in ("f32", "f16")}
-        if world == 1 and args.sweep_steps > 0:
-            line["batched"] = bench_sweep(args, dev, peak)
-        if world == 1 and args.serve_requests > 0:
-            line["served"] = bench_served(args, dev)
+        line.update(extra)
         if cpu_line is not None:
             line["cpu_baseline"] = cpu_line
         print(json.dumps(line), flush=True)

@@ -50,6 +50,14 @@ class Replicas:
         """Whole-job rate: the units every rank processed over the slowest rank's time."""
         return self.sum(units) / max(self.max(seconds), 1e-300)
 
+    def gather(self, obj):
+        """Every rank's `obj` (a picklable host value), in rank order, on every rank."""
+        if self.world == 1:
+            return [obj]
+        out = [None] * self.world
+        dist.all_gather_object(out, obj)
+        return out
+
     def share(self, items):
         """This rank's share of a list of independent items (round robin, so sizes spread evenly)."""
         return list(items)[self.rank::self.world]

@@ -26,8 +26,12 @@ def worker(rank, world, port, q):
         rep.barrier()
         seconds = [2.0, 3.5][rank]
         units = [100.0, 300.0][rank]
+        # a sweep shared out: each rank runs its specs, the per-rank results are assembled on every rank
+        from cerebrosim_b200 import workloads
+        mine = rep.share(workloads.sweep())
+        done = [{"seed": sp["seed"], "nodes": sp["nodes"], "rank": rep.rank} for sp in mine]
         out = {"rank": rep.rank, "world": rep.world, "max": rep.max(seconds), "sum": rep.sum(units),
-               "rate": rep.rate(units, seconds), "share": rep.share(range(7))}
+               "rate": rep.rate(units, seconds), "share": rep.share(range(7)), "gathered": rep.gather(done)}
         rep.barrier()
         q.put(out)
     finally:
@@ -50,6 +54,12 @@ def test_two_replicas_over_gloo():
         assert r["max"] == 3.5 and r["sum"] == 400.0
         assert r["rate"] == pytest.approx(400.0 / 3.5)
     assert res[0]["share"] == [0, 2, 4, 6] and res[1]["share"] == [1, 3, 5]
+    # every spec of the sweep ran on exactly one rank, and both ranks hold the same assembled list
+    from cerebrosim_b200 import workloads
+    assert res[0]["gathered"] == res[1]["gathered"]
+    ran = sorted(d["seed"] for part in res[0]["gathered"] for d in part)
+    assert ran == sorted(sp["seed"] for sp in workloads.sweep())
+    assert [d["rank"] for d in res[0]["gathered"][1]] == [1] * len(res[0]["gathered"][1])
 
 
 def test_single_process_is_a_plain_run(monkeypatch):
