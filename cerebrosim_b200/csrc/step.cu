@@ -277,11 +277,7 @@ template <int ST> struct PopV<ST, float> {
     }
 };
 template <int ST> struct PopV<ST, float2> {
-    static __device__ __forceinline__ void st_scaled(void* b, uint32_t idx, float2 g) {
-        if constexpr (ST == CS_STORE_F32) *reinterpret_cast<float2*>(static_cast<float*>(b) + idx) = g;
-        else if constexpr (ST == CS_STORE_F16) *reinterpret_cast<__half2*>(static_cast<__half*>(b) + idx) = __float22half2_rn(g);
-        else *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(b) + idx) = __float22bfloat162_rn(g);
-    }
+    static __device__ __forceinline__ void st_scaled(void* b, uint32_t idx, float2 g);   // after Pop2, below
 };
 
 // One pair's outputs: FP32 stores w (A + e +- o); the 16-bit formats store (f - w) 1024 / w = 1024 (A + e +- o),
@@ -879,34 +875,79 @@ __global__ void __launch_bounds__(DENSE_BLOCK, DENSE_MIN_BLOCKS) k_bulk_dense(co
 // which path took it. Needs an even population row length (the pair stores are aligned) and no outlet coupling
 // (the flux partition is per block of `block` nodes); the host selects it only then.
 constexpr int PAIR_BLOCK = 128;
-constexpr int PAIR_MIN_BLOCKS = 5;
+#ifndef CS_PAIR_MIN_BLOCKS
+#define CS_PAIR_MIN_BLOCKS 5
+#endif
+#ifndef CS_PAIR_STRIDE
+#define CS_PAIR_STRIDE 32
+#endif
+constexpr int PAIR_MIN_BLOCKS = CS_PAIR_MIN_BLOCKS;
+// Distance between a thread's two nodes: 32 (a warp takes 64 consecutive nodes, lane t nodes t and t + 32, so every
+// load and store of the warp covers 32 consecutive elements) or 1 (nodes 2t and 2t + 1: paired 64/32-bit stores,
+// but every load instruction touches each sector twice).
+constexpr int PAIR_STRIDE = CS_PAIR_STRIDE;
+static_assert(PAIR_STRIDE == 1 || PAIR_STRIDE == 32, "pair stride");
 
-template <int ST> struct Pop2;
-template <> struct Pop2<CS_STORE_F32> {
+// Two populations at idx and idx + S, scaled to f - w (float2: the pair's two nodes).
+template <int ST, int S> struct Pop2;
+template <int S> struct Pop2<CS_STORE_F32, S> {
     static __device__ __forceinline__ float2 ld(const void* b, uint32_t idx, float) {
         const float* p = static_cast<const float*>(b) + idx;
-        return make_float2(__ldg(p), __ldg(p + 1));
+        return make_float2(__ldg(p), __ldg(p + S));
+    }
+    static __device__ __forceinline__ void st(void* b, uint32_t idx, float2 g) {
+        float* p = static_cast<float*>(b) + idx;
+        if constexpr (S == 1) {
+            *reinterpret_cast<float2*>(p) = g;
+        } else {
+            p[0] = g.x;
+            p[S] = g.y;
+        }
     }
 };
-template <> struct Pop2<CS_STORE_F16> {
+template <int S> struct Pop2<CS_STORE_F16, S> {
     static __device__ __forceinline__ float2 ld(const void* b, uint32_t idx, float w) {
         const __half* p = static_cast<const __half*>(b) + idx;
-        return VO<float2>::mul(make_float2(__half2float(__ldg(p)), __half2float(__ldg(p + 1))),
+        return VO<float2>::mul(make_float2(__half2float(__ldg(p)), __half2float(__ldg(p + S))),
                                VO<float2>::k(w * (1.0f / 1024.0f)));
     }
+    static __device__ __forceinline__ void st(void* b, uint32_t idx, float2 g) {
+        __half* p = static_cast<__half*>(b) + idx;
+        if constexpr (S == 1) {
+            *reinterpret_cast<__half2*>(p) = __float22half2_rn(g);
+        } else {
+            p[0] = __float2half_rn(g.x);
+            p[S] = __float2half_rn(g.y);
+        }
+    }
 };
-template <> struct Pop2<CS_STORE_BF16> {
+template <int S> struct Pop2<CS_STORE_BF16, S> {
     static __device__ __forceinline__ float2 ld(const void* b, uint32_t idx, float w) {
         const __nv_bfloat16* p = static_cast<const __nv_bfloat16*>(b) + idx;
-        return VO<float2>::mul(make_float2(__bfloat162float(__ldg(p)), __bfloat162float(__ldg(p + 1))),
+        return VO<float2>::mul(make_float2(__bfloat162float(__ldg(p)), __bfloat162float(__ldg(p + S))),
                                VO<float2>::k(w * (1.0f / 1024.0f)));
+    }
+    static __device__ __forceinline__ void st(void* b, uint32_t idx, float2 g) {
+        __nv_bfloat16* p = static_cast<__nv_bfloat16*>(b) + idx;
+        if constexpr (S == 1) {
+            *reinterpret_cast<__nv_bfloat162*>(p) = __float22bfloat162_rn(g);
+        } else {
+            p[0] = __float2bfloat16_rn(g.x);
+            p[S] = __float2bfloat16_rn(g.y);
+        }
     }
 };
 
-// Nodes n (even) and n + 1, both regular in segment `code`.
+template <int ST>
+__device__ __forceinline__ void PopV<ST, float2>::st_scaled(void* b, uint32_t idx, float2 g) {
+    Pop2<ST, PAIR_STRIDE>::st(b, idx, g);
+}
+
+// Nodes n and n + PAIR_STRIDE, both regular in segment `code`.
 template <int ST, bool GAL>
 __device__ __forceinline__ void pair_update(const cs_step_desc& d, const int a, const int32_t n, const int32_t code) {
     using O = VO<float2>;
+    constexpr int S = PAIR_STRIDE;
     const int32_t N = int32_t(d.n);
     const uint32_t NP = uint32_t(d.npad);
     const void* fin = d.f[a];
@@ -924,7 +965,7 @@ __device__ __forceinline__ void pair_update(const cs_step_desc& d, const int a, 
         if (4 * k + 2 < Q) lk[4 * k + 2] = n + v.z;
         if (4 * k + 3 < Q) lk[4 * k + 3] = n + v.w;
     }
-    const float2 om = __ldg(reinterpret_cast<const float2*>(d.om + n));
+    const float2 om = make_float2(__ldg(d.om + n), __ldg(d.om + n + S));
     grid_dependency_wait();
     // the six axis neighbours' previous velocity (fluid for a regular node) for the Galilean differences
     float2 g[6];
@@ -932,13 +973,13 @@ __device__ __forceinline__ void pair_update(const cs_step_desc& d, const int a, 
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             const float* p = vin + int64_t(k / 2) * N + lk[1 + k];
-            g[k] = make_float2(__ldg(p), __ldg(p + 1));
+            g[k] = make_float2(__ldg(p), __ldg(p + S));
         }
     }
     float2 fk[Q];
     Unroll<0, Q>::run([&](auto ic) {
         constexpr int I = decltype(ic)::value;
-        fk[I] = Pop2<ST>::ld(fin, uint32_t(I) * NP + uint32_t(lk[I]), wgt(I));
+        fk[I] = Pop2<ST, S>::ld(fin, uint32_t(I) * NP + uint32_t(lk[I]), wgt(I));
     });
     Moments<float2> m;
     moments27(fk, m);
@@ -950,26 +991,33 @@ __device__ __forceinline__ void pair_update(const cs_step_desc& d, const int a, 
     }
     regularised_out<ST, GAL, float2>(fout, NP, n, m.dr, om, t);
     vout[n] = t.ux.x;
-    vout[n + 1] = t.ux.y;
+    vout[n + S] = t.ux.y;
     vout[N + n] = t.uy.x;
-    vout[N + n + 1] = t.uy.y;
+    vout[N + n + S] = t.uy.y;
     vout[2 * N + n] = t.uz.x;
-    vout[2 * N + n + 1] = t.uz.y;
-    *reinterpret_cast<float2*>(d.rho + n) = m.dr;
+    vout[2 * N + n + S] = t.uz.y;
+    d.rho[n] = m.dr.x;
+    d.rho[n + S] = m.dr.y;
 }
 
 template <int ST, bool GAL>
 __global__ void __launch_bounds__(PAIR_BLOCK, PAIR_MIN_BLOCKS) k_bulk_pair(const cs_step_desc d, const int a) {
-    const int32_t n = 2 * (int32_t(blockIdx.x) * int32_t(blockDim.x) + int32_t(threadIdx.x));
+    constexpr int S = PAIR_STRIDE;
+    const int32_t t = int32_t(blockIdx.x) * int32_t(blockDim.x) + int32_t(threadIdx.x);
+    // stride 1: nodes 2t, 2t + 1; stride 32: warp w's 64 nodes from 64 w, lane l takes l and l + 32
+    const int32_t n = S == 1 ? 2 * t : 64 * (t >> 5) + (t & 31);
     if (n < d.n) {
-        int2 c = make_int2(-1, -1);
-        if (n + 1 < d.n) c = __ldg(reinterpret_cast<const int2*>(d.lcode + n));
-        if (c.x >= 0 && c.x == c.y) {
-            pair_update<ST, GAL>(d, a, n, c.x);
+        int32_t c0 = -1, c1 = -2;
+        if (n + S < d.n) {
+            c0 = __ldg(d.lcode + n);
+            c1 = __ldg(d.lcode + n + S);
+        }
+        if (c0 >= 0 && c0 == c1) {
+            pair_update<ST, GAL>(d, a, n, c0);
         } else {
             float ux, uy, uz;
             node_update<ST, CS_MODEL_REGULARISED, GAL, false>(d, a, n, ux, uy, uz);
-            if (n + 1 < d.n) node_update<ST, CS_MODEL_REGULARISED, GAL, false>(d, a, n + 1, ux, uy, uz);
+            if (n + S < d.n) node_update<ST, CS_MODEL_REGULARISED, GAL, false>(d, a, n + S, ux, uy, uz);
         }
     }
     grid_dependency_wait();
@@ -1040,7 +1088,7 @@ bool use_pairs(const cs_step_desc& d) {
     const bool force = d.force[0] != 0.0f || d.force[1] != 0.0f || d.force[2] != 0.0f;
     const int block = d.block ? d.block : MAX_BLOCK;
     return d.model == CS_MODEL_REGULARISED && !force && d.sigma >= 1.0f && d.n_open == 0 && block <= PAIR_BLOCK &&
-           d.npad % 2 == 0;
+           (PAIR_STRIDE != 1 || d.npad % 2 == 0);
 }
 
 template <int ST>

@@ -225,7 +225,7 @@ def pressure_ends(g):
 
 
 def calibrated_solver(spec, dx_mm=None, storage="f32", block=None, device=None, order="c", steps_per_beat=8000,
-                      tau=0.52, pref_lu=0.004, target_share=135.0 / 240.0, relax_steps=100, sponge=(8, 0.6)):
+                      tau=0.52, pref_lu=0.002, target_share=135.0 / 240.0, relax_steps=100, sponge=(8, 0.6)):
     """A generated vessel run as simulate.run runs the reference's arteries (simulate.py:253-337): pressure inlet
     driven by the lumped circuit's inlet pressure, resistance outlets relaxed towards R Q - pref, flow measured on
     slabs inside each end, and the inlet pressure recalibrated after every beat from the beat's mean inlet pressure

@@ -129,8 +129,11 @@ def test_diverged_request_is_evicted_and_the_others_are_unchanged():
         assert np.array_equal(alone.fields[0], r.fields[0]) and np.array_equal(alone.fields[1], r.fields[1]), r.id
 
 
+SPB_CAL = 2000      # steps per beat of the calibrated requests: long enough for the inflow to cross the vessel
+
+
 def calibrated_specs():
-    return [{"id": k, "arrival": 0.0, "seed": 300 + k, "stenosis": s, "pressure": p, "beats": 3, "nodes": n}
+    return [{"id": k, "arrival": 0.0, "seed": 300 + k, "stenosis": s, "pressure": p, "beats": 2, "nodes": n}
             for k, (s, p, n) in enumerate([(0.5, 90.0, 30e3), (0.0, 120.0, 45e3), (0.7, 75.0, 25e3)])]
 
 
@@ -145,17 +148,18 @@ def test_served_recalibration_matches_dedicated_artery_solver():
         serve.recalibrate_on_beat(r, beat)
         seen[(r.id, beat)] = dict(r.solver.calibration.history[-1])
 
-    sv = server("f32", max_active=3, builder=workloads.calibrated_builder, on_beat=hook)
+    sv = server("f32", max_active=3, builder=workloads.calibrated_builder, on_beat=hook, steps_per_beat=SPB_CAL,
+                chunk=500, graph_chunk=100)
     mix = sv.serve(calibrated_specs(), realtime=False)
-    assert all(r.ok for r in mix)
+    assert all(r.ok for r in mix), [(r.id, r.evicted) for r in mix]
     for r in mix:
-        s = workloads.calibrated_solver(r.spec, storage="f32", block=128, steps_per_beat=SPB)
+        s = workloads.calibrated_solver(r.spec, storage="f32", block=128, steps_per_beat=SPB_CAL)
         for b in range(1, r.beats + 1):
-            s.run(SPB, chunk=50)
+            s.run(SPB_CAL, chunk=100)
             if b < r.beats:
                 s.calibration.on_beat(b)
                 h, hs = s.calibration.history[-1], seen[(r.id, b)]
-                assert h["steps"] == hs["steps"] == SPB
+                assert h["steps"] == hs["steps"] == SPB_CAL
                 assert h["R_seg"] == pytest.approx(hs["R_seg"], rel=1e-6, abs=1.0)
                 assert h["q_in_ml_min"] == pytest.approx(hs["q_in_ml_min"], rel=1e-6)
         p, u = s.fields()
