@@ -109,7 +109,7 @@ __device__ __forceinline__ float weight_rt(int i) {
 // source, the ghost slot's gq for a boundary link (q >= 0: wall at distance max(q, 0.1) with u = 0; -1: an opening,
 // u = u0 at distance 1). Two fluid neighbours (the common case) give the central difference (v2 - v1) / 2.
 __device__ __forceinline__ float ddx_g(int32_t sm, int32_t sp, float gm, float gp, float u0, int32_t n_nodes) {
-    if (sm < n_nodes && sp < n_nodes) return __fmul_rn(0.5f, __fsub_rn(gp, gm));   // as the node-pair path
+    if (sm < n_nodes && sp < n_nodes) return 0.5f * (gp - gm);
     float h1 = 1.0f, v1 = u0, h2 = 1.0f, v2 = u0;
     if (sm < n_nodes) {
         v1 = gm;
@@ -169,34 +169,25 @@ struct Unroll<N_, N_> {
     static __device__ __forceinline__ void run(F&&) {}
 };
 
-// ---- arithmetic with explicit rounding on one node (float) or on two nodes at once (float2) ---------------------------
-// The regularised step below is written once over V = float or V = float2; float2 uses sm_100's packed FP32x2
-// instructions (one instruction for both nodes). Every operation is an explicitly rounded intrinsic (no implicit
-// multiply-add contraction), so a node gets the same bits whether it is updated alone or as half of a pair.
-template <class V> struct VO;
-template <> struct VO<float> {
-    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
-    static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
-    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
-    static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-    static __device__ __forceinline__ float k(float x) { return x; }
-    static __device__ __forceinline__ float rcp(float a) { return __frcp_rn(a); }
-};
-template <> struct VO<float2> {
-    static __device__ __forceinline__ float2 add(float2 a, float2 b) { return __fadd2_rn(a, b); }
-    // a - b as b * (-1) + a: one rounding of the exact difference, as __fsub_rn
-    static __device__ __forceinline__ float2 sub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
-    static __device__ __forceinline__ float2 mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
-    static __device__ __forceinline__ float2 fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-    static __device__ __forceinline__ float2 k(float x) { return make_float2(x, x); }
-    static __device__ __forceinline__ float2 rcp(float2 a) { return make_float2(__frcp_rn(a.x), __frcp_rn(a.y)); }
-};
-
 // Moment sums from pulled values; a pair (I, opp(I)) enters through its sum s and difference dd.
-template <class V = float>
 struct Moments {
-    V dr, jx, jy, jz;
-    V pxx, pyy, pzz, pxy, pxz, pyz;
+    float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+    float pxx = 0.f, pyy = 0.f, pzz = 0.f, pxy = 0.f, pxz = 0.f, pyz = 0.f;
+    template <int I>
+    __device__ __forceinline__ void add_pair(float v, float vo) {
+        constexpr int x = Lat::cx(I), y = Lat::cy(I), z = Lat::cz(I);
+        const float s = v + vo, dd = v - vo;
+        dr += s;
+        if (x) jx += x * dd;
+        if (y) jy += y * dd;
+        if (z) jz += z * dd;
+        if (x) pxx += s;
+        if (y) pyy += s;
+        if (z) pzz += s;
+        if (x && y) pxy += (x * y) * s;
+        if (x && z) pxz += (x * z) * s;
+        if (y && z) pyz += (y * z) * s;
+    }
 };
 
 // c^T M c for link I with M given by its diagonal and twice its off-diagonal entries.
@@ -239,62 +230,44 @@ static_assert(pair_is(19, 1, 1, 1) && pair_is(21, 1, 1, -1) && pair_is(23, 1, -1
 // its sum s and difference d, and the terms several moments share are added once — the three edge planes, and the
 // four corner pairs through a butterfly (their sums give the trace and the three off-diagonals of Pi, their
 // differences the corner parts of j). 81 additions instead of 111 for the link-by-link sums.
-template <class V>
-__device__ __forceinline__ void moments27(const V (&f)[Q], Moments<V>& m) {
-    using O = VO<V>;
-    V sp[Q / 2 + 1], dp[Q / 2 + 1];
+__device__ __forceinline__ void moments27(const float (&f)[Q], Moments& m) {
+    float sp[Q / 2 + 1], dp[Q / 2 + 1];
 #pragma unroll
     for (int k = 0; k < 13; ++k) {
-        sp[k] = O::add(f[1 + 2 * k], f[2 + 2 * k]);
-        dp[k] = O::sub(f[1 + 2 * k], f[2 + 2 * k]);
+        sp[k] = f[1 + 2 * k] + f[2 + 2 * k];
+        dp[k] = f[1 + 2 * k] - f[2 + 2 * k];
     }
     // pair k holds links 1 + 2k and 2 + 2k: k = 0, 1, 2 axis; 3 .. 8 edges; 9 .. 12 corners
-    const V exy = O::add(sp[3], sp[4]), exz = O::add(sp[5], sp[6]), eyz = O::add(sp[7], sp[8]);
-    const V ca = O::add(sp[9], sp[10]), cb = O::sub(sp[9], sp[10]), cc = O::add(sp[11], sp[12]);
-    const V ce = O::sub(sp[11], sp[12]);
-    const V sc = O::add(ca, cc);
-    m.dr = O::add(O::add(O::add(O::add(O::add(O::add(O::add(f[0], sp[0]), sp[1]), sp[2]), exy), exz), eyz), sc);
-    m.pxx = O::add(O::add(O::add(sp[0], exy), exz), sc);
-    m.pyy = O::add(O::add(O::add(sp[1], exy), eyz), sc);
-    m.pzz = O::add(O::add(O::add(sp[2], exz), eyz), sc);
-    m.pxy = O::add(O::sub(sp[3], sp[4]), O::sub(ca, cc));
-    m.pxz = O::add(O::sub(sp[5], sp[6]), O::add(cb, ce));
-    m.pyz = O::add(O::sub(sp[7], sp[8]), O::sub(cb, ce));
-    const V dpp = O::add(dp[9], dp[10]), dpr = O::sub(dp[9], dp[10]), dpt = O::add(dp[11], dp[12]);
-    const V dpv = O::sub(dp[11], dp[12]);
-    m.jx = O::add(O::add(O::add(O::add(O::add(dp[0], dp[3]), dp[4]), dp[5]), dp[6]), O::add(dpp, dpv));
-    m.jy = O::add(O::add(O::add(O::sub(O::add(dp[1], dp[3]), dp[4]), dp[7]), dp[8]), O::sub(dpp, dpv));
-    m.jz = O::add(O::sub(O::add(O::sub(O::add(dp[2], dp[5]), dp[6]), dp[7]), dp[8]), O::add(dpr, dpt));
+    const float exy = sp[3] + sp[4], exz = sp[5] + sp[6], eyz = sp[7] + sp[8];
+    const float ca = sp[9] + sp[10], cb = sp[9] - sp[10], cc = sp[11] + sp[12], ce = sp[11] - sp[12];
+    const float sc = ca + cc;
+    m.dr = f[0] + sp[0] + sp[1] + sp[2] + exy + exz + eyz + sc;
+    m.pxx = sp[0] + exy + exz + sc;
+    m.pyy = sp[1] + exy + eyz + sc;
+    m.pzz = sp[2] + exz + eyz + sc;
+    m.pxy = (sp[3] - sp[4]) + (ca - cc);
+    m.pxz = (sp[5] - sp[6]) + (cb + ce);
+    m.pyz = (sp[7] - sp[8]) + (cb - ce);
+    const float dpp = dp[9] + dp[10], dpr = dp[9] - dp[10], dpt = dp[11] + dp[12], dpv = dp[11] - dp[12];
+    m.jx = dp[0] + dp[3] + dp[4] + dp[5] + dp[6] + (dpp + dpv);
+    m.jy = dp[1] + dp[3] - dp[4] + dp[7] + dp[8] + (dpp - dpv);
+    m.jz = dp[2] + dp[5] - dp[6] + dp[7] - dp[8] + (dpr + dpt);
 }
-
-// Population store of one value (V = float) or of two consecutive nodes' values (V = float2; the first node's index
-// is even and so is the row length, so the pair is one aligned 64-bit FP32 or 32-bit 16-bit store).
-template <int ST, class V> struct PopV;
-template <int ST> struct PopV<ST, float> {
-    static __device__ __forceinline__ void st_scaled(void* b, uint32_t idx, float g) {
-        if constexpr (ST == CS_STORE_F32) static_cast<float*>(b)[idx] = g;
-        else Pop<ST>::st_scaled(b, idx, g);
-    }
-};
-template <int ST> struct PopV<ST, float2> {
-    static __device__ __forceinline__ void st_scaled(void* b, uint32_t idx, float2 g);   // after Pop2, below
-};
 
 // One pair's outputs: FP32 stores w (A + e +- o); the 16-bit formats store (f - w) 1024 / w = 1024 (A + e +- o),
 // for which A, e and o arrive already multiplied by 1024 (no per-link weight or scale left to apply).
-template <int ST, int I, class V>
-__device__ __forceinline__ void store_pair(void* fout, uint32_t NP, int32_t n, V A, V e, V o) {
-    using O = VO<V>;
-    constexpr int OP = Lat::opp(I);
+template <int ST, int I>
+__device__ __forceinline__ void store_pair(void* fout, uint32_t NP, int32_t n, float A, float e, float o) {
+    constexpr int O = Lat::opp(I);
     if constexpr (ST == CS_STORE_F32) {
         constexpr float w = wgt(I);
-        const V wb = O::mul(O::k(w), O::add(A, e));
-        PopV<ST, V>::st_scaled(fout, uint32_t(I) * NP + uint32_t(n), O::fma(O::k(w), o, wb));
-        PopV<ST, V>::st_scaled(fout, uint32_t(OP) * NP + uint32_t(n), O::fma(O::k(-w), o, wb));
+        const float wb = w * (A + e);
+        Pop<ST>::st(fout, uint32_t(I) * NP + uint32_t(n), w, fmaf(w, o, wb));
+        Pop<ST>::st(fout, uint32_t(O) * NP + uint32_t(n), w, fmaf(-w, o, wb));
     } else {
-        const V b = O::add(A, e);
-        PopV<ST, V>::st_scaled(fout, uint32_t(I) * NP + uint32_t(n), O::add(b, o));
-        PopV<ST, V>::st_scaled(fout, uint32_t(OP) * NP + uint32_t(n), O::sub(b, o));
+        const float b = A + e;
+        Pop<ST>::st_scaled(fout, uint32_t(I) * NP + uint32_t(n), b + o);
+        Pop<ST>::st_scaled(fout, uint32_t(O) * NP + uint32_t(n), b - o);
     }
 }
 
@@ -302,129 +275,68 @@ __device__ __forceinline__ void store_pair(void* fout, uint32_t NP, int32_t n, V
 // f_opp = w_I (A + e_I - o_I), with e_I = c_I^T M c_I for M = 4.5 u u^T + 4.5 (1 - om) P' (given as its diagonal
 // and twice its off-diagonal: m*) and o_I = 3 c_I . u + h3_I (the third-order term, with the Galilean model). Axis,
 // edge and corner links differ only in signs, so the 13 pairs' e and o come from shared partial sums.
-template <int ST, bool GAL, class V>
-__device__ __forceinline__ void store_regularised(void* fout, uint32_t NP, int32_t n, V A, V ux, V uy, V uz, V mxx,
-                                                  V myy, V mzz, V mxy2, V mxz2, V myz2) {
-    using O = VO<V>;
+template <int ST, bool GAL>
+__device__ __forceinline__ void store_regularised(void* fout, uint32_t NP, int32_t n, float A, float ux, float uy,
+                                                  float uz, float mxx, float myy, float mzz, float mxy2,
+                                                  float mxz2, float myz2) {
     // SC: the stored scale (1024 for the 16-bit formats, applied to A, M and the constants; exact in binary)
     constexpr float SC = ST == CS_STORE_F32 ? 1.0f : 1024.0f;
     if constexpr (ST == CS_STORE_F32) {
-        PopV<ST, V>::st_scaled(fout, uint32_t(n), O::mul(O::k(wgt(0)), A));
+        Pop<ST>::st(fout, uint32_t(n), wgt(0), wgt(0) * A);
     } else {
-        A = O::mul(A, O::k(SC));
-        mxx = O::mul(mxx, O::k(SC));
-        myy = O::mul(myy, O::k(SC));
-        mzz = O::mul(mzz, O::k(SC));
-        mxy2 = O::mul(mxy2, O::k(SC));
-        mxz2 = O::mul(mxz2, O::k(SC));
-        myz2 = O::mul(myz2, O::k(SC));
-        PopV<ST, V>::st_scaled(fout, uint32_t(n), A);
+        A *= SC;
+        mxx *= SC;
+        myy *= SC;
+        mzz *= SC;
+        mxy2 *= SC;
+        mxz2 *= SC;
+        myz2 *= SC;
+        Pop<ST>::st_scaled(fout, uint32_t(n), A);
     }
-    // o_I = 3 c.u + h3_I; the third-order terms come from the velocity monomials: axis links -4.5 (sum of two),
-    // edges 9 (..) - 4.5 (..), corners 9 (+-A1 +-A2 +-A3) +- 27 xyz
-    const V t3 = O::k(3.0f * SC);
-    V o1, o3, o5, o7, o9, o11, o13, o15, o17, o19, o21, o23, o25;
-    const V u7 = O::add(ux, uy), u9 = O::sub(ux, uy);
-    const V u11 = O::add(ux, uz), u13 = O::sub(ux, uz), u15 = O::add(uy, uz), u17 = O::sub(uy, uz);
-    const V u19 = O::add(u7, uz), u21 = O::sub(u7, uz), u23 = O::add(u9, uz), u25 = O::sub(uz, u9);
-    if constexpr (GAL) {
-        const V x2 = O::mul(ux, ux), y2 = O::mul(uy, uy), z2 = O::mul(uz, uz);
-        const V xxy = O::mul(x2, uy), xxz = O::mul(x2, uz), xyy = O::mul(ux, y2), yyz = O::mul(y2, uz);
-        const V xzz = O::mul(ux, z2), yzz = O::mul(uy, z2);
-        const V xyz = O::mul(O::mul(ux, uy), uz);
-        const V a1 = O::add(xxy, yzz), a2 = O::add(xxz, yyz), a3 = O::add(xyy, xzz);
-        const V n45 = O::k(-4.5f * SC), p45 = O::k(4.5f * SC), p9 = O::k(9.0f * SC);
-        o1 = O::fma(t3, ux, O::mul(n45, a3));
-        o3 = O::fma(t3, uy, O::mul(n45, a1));
-        o5 = O::fma(t3, uz, O::mul(n45, a2));
-        o7 = O::fma(t3, u7, O::sub(O::mul(p9, O::add(xyy, xxy)), O::mul(p45, O::add(xzz, yzz))));
-        o9 = O::fma(t3, u9, O::sub(O::mul(p9, O::sub(xyy, xxy)), O::mul(p45, O::sub(xzz, yzz))));
-        o11 = O::fma(t3, u11, O::sub(O::mul(p9, O::add(xzz, xxz)), O::mul(p45, O::add(xyy, yyz))));
-        o13 = O::fma(t3, u13, O::sub(O::mul(p9, O::sub(xzz, xxz)), O::mul(p45, O::sub(xyy, yyz))));
-        o15 = O::fma(t3, u15, O::sub(O::mul(p9, O::add(yzz, yyz)), O::mul(p45, O::add(xxy, xxz))));
-        o17 = O::fma(t3, u17, O::sub(O::mul(p9, O::sub(yzz, yyz)), O::mul(p45, O::sub(xxy, xxz))));
-        const V b1 = O::mul(p9, a1), b2 = O::mul(p9, a2), b3 = O::mul(p9, a3);
-        const V bx = O::mul(O::k(27.0f * SC), xyz);
-        const V p_ = O::add(b1, b3), q_ = O::add(b2, bx), m_ = O::sub(b3, b1), n_ = O::sub(b2, bx);
-        o19 = O::fma(t3, u19, O::add(p_, q_));
-        o21 = O::fma(t3, u21, O::sub(p_, q_));
-        o23 = O::fma(t3, u23, O::add(m_, n_));
-        o25 = O::fma(t3, u25, O::sub(n_, m_));
-    } else {
-        o1 = O::mul(t3, ux), o3 = O::mul(t3, uy), o5 = O::mul(t3, uz);
-        o7 = O::mul(t3, u7), o9 = O::mul(t3, u9), o11 = O::mul(t3, u11), o13 = O::mul(t3, u13);
-        o15 = O::mul(t3, u15), o17 = O::mul(t3, u17);
-        o19 = O::mul(t3, u19), o21 = O::mul(t3, u21), o23 = O::mul(t3, u23), o25 = O::mul(t3, u25);
+    // third-order terms from the velocity monomials: axis links -4.5 (sum of two), edges 9 (..) - 4.5 (..),
+    // corners 9 (+-A1 +-A2 +-A3) +- 27 xyz
+    float h1 = 0.f, h3 = 0.f, h5 = 0.f, h7 = 0.f, h9 = 0.f, h11 = 0.f, h13 = 0.f, h15 = 0.f, h17 = 0.f;
+    float h19 = 0.f, h21 = 0.f, h23 = 0.f, h25 = 0.f;
+    if (GAL) {
+        const float x2 = ux * ux, y2 = uy * uy, z2 = uz * uz;
+        const float xxy = x2 * uy, xxz = x2 * uz, xyy = ux * y2, yyz = y2 * uz, xzz = ux * z2, yzz = uy * z2;
+        const float xyz = ux * uy * uz;
+        const float a1 = xxy + yzz, a2 = xxz + yyz, a3 = xyy + xzz;
+        h1 = (-4.5f * SC) * a3;
+        h3 = (-4.5f * SC) * a1;
+        h5 = (-4.5f * SC) * a2;
+        h7 = (9.0f * SC) * (xyy + xxy) - (4.5f * SC) * (xzz + yzz);
+        h9 = (9.0f * SC) * (xyy - xxy) - (4.5f * SC) * (xzz - yzz);
+        h11 = (9.0f * SC) * (xzz + xxz) - (4.5f * SC) * (xyy + yyz);
+        h13 = (9.0f * SC) * (xzz - xxz) - (4.5f * SC) * (xyy - yyz);
+        h15 = (9.0f * SC) * (yzz + yyz) - (4.5f * SC) * (xxy + xxz);
+        h17 = (9.0f * SC) * (yzz - yyz) - (4.5f * SC) * (xxy - xxz);
+        const float b1 = (9.0f * SC) * a1, b2 = (9.0f * SC) * a2, b3 = (9.0f * SC) * a3, bx = (27.0f * SC) * xyz;
+        const float p_ = b1 + b3, q_ = b2 + bx, m_ = b3 - b1, n_ = b2 - bx;
+        h19 = p_ + q_;
+        h21 = p_ - q_;
+        h23 = m_ + n_;
+        h25 = n_ - m_;
     }
     // axis
-    store_pair<ST, 1>(fout, NP, n, A, mxx, o1);
-    store_pair<ST, 3>(fout, NP, n, A, myy, o3);
-    store_pair<ST, 5>(fout, NP, n, A, mzz, o5);
+    store_pair<ST, 1>(fout, NP, n, A, mxx, (3.0f * SC) * ux + h1);
+    store_pair<ST, 3>(fout, NP, n, A, myy, (3.0f * SC) * uy + h3);
+    store_pair<ST, 5>(fout, NP, n, A, mzz, (3.0f * SC) * uz + h5);
     // edges, plane by plane
-    const V sxy = O::add(mxx, myy), sxz = O::add(mxx, mzz), syz = O::add(myy, mzz);
-    store_pair<ST, 7>(fout, NP, n, A, O::add(sxy, mxy2), o7);
-    store_pair<ST, 9>(fout, NP, n, A, O::sub(sxy, mxy2), o9);
-    store_pair<ST, 11>(fout, NP, n, A, O::add(sxz, mxz2), o11);
-    store_pair<ST, 13>(fout, NP, n, A, O::sub(sxz, mxz2), o13);
-    store_pair<ST, 15>(fout, NP, n, A, O::add(syz, myz2), o15);
-    store_pair<ST, 17>(fout, NP, n, A, O::sub(syz, myz2), o17);
+    const float sxy = mxx + myy, sxz = mxx + mzz, syz = myy + mzz;
+    const float u7 = ux + uy, u9 = ux - uy;
+    store_pair<ST, 7>(fout, NP, n, A, sxy + mxy2, (3.0f * SC) * u7 + h7);
+    store_pair<ST, 9>(fout, NP, n, A, sxy - mxy2, (3.0f * SC) * u9 + h9);
+    store_pair<ST, 11>(fout, NP, n, A, sxz + mxz2, (3.0f * SC) * (ux + uz) + h11);
+    store_pair<ST, 13>(fout, NP, n, A, sxz - mxz2, (3.0f * SC) * (ux - uz) + h13);
+    store_pair<ST, 15>(fout, NP, n, A, syz + myz2, (3.0f * SC) * (uy + uz) + h15);
+    store_pair<ST, 17>(fout, NP, n, A, syz - myz2, (3.0f * SC) * (uy - uz) + h17);
     // corners
-    const V tr = O::add(sxy, mzz), ca = O::add(tr, mxy2), cb = O::sub(tr, mxy2);
-    const V cg = O::add(mxz2, myz2), cd = O::sub(mxz2, myz2);
-    store_pair<ST, 19>(fout, NP, n, A, O::add(ca, cg), o19);
-    store_pair<ST, 21>(fout, NP, n, A, O::sub(ca, cg), o21);
-    store_pair<ST, 23>(fout, NP, n, A, O::add(cb, cd), o23);
-    store_pair<ST, 25>(fout, NP, n, A, O::sub(cb, cd), o25);
-}
-
-// The regularised step without a body force from the moments on (lbm.py:183-204, 217-240), for one node or two:
-// velocity u = j, the regularised non-equilibrium stress P = Pi - dr/3 I - u u^T (by the D3Q27 isotropy
-// sum_i w_i c c^T feq2_i = dr/3 I + u u^T), minus the Galilean correction diag(Ed) (Ed_a = 3 tau u_a^2 du_a/dx_a from
-// the given differences), then the outputs w_i (A + e_i +- o_i). `hybrid` (single nodes only) may replace P by the
-// hybrid blend (lbm.py:224-229) before the correction.
-template <class V>
-struct Stress {
-    V ux, uy, uz, usq, pxx, pyy, pzz, pxy, pxz, pyz;
-};
-
-template <class V>
-__device__ __forceinline__ Stress<V> regularised_stress(const Moments<V>& m) {
-    using O = VO<V>;
-    Stress<V> t;
-    t.ux = m.jx, t.uy = m.jy, t.uz = m.jz;
-    t.usq = O::fma(t.uz, t.uz, O::fma(t.uy, t.uy, O::mul(t.ux, t.ux)));
-    const V d3 = O::mul(m.dr, O::k(1.0f / 3.0f));
-    t.pxx = O::sub(O::sub(m.pxx, d3), O::mul(t.ux, t.ux));
-    t.pyy = O::sub(O::sub(m.pyy, d3), O::mul(t.uy, t.uy));
-    t.pzz = O::sub(O::sub(m.pzz, d3), O::mul(t.uz, t.uz));
-    t.pxy = O::sub(m.pxy, O::mul(t.ux, t.uy));
-    t.pxz = O::sub(m.pxz, O::mul(t.ux, t.uz));
-    t.pyz = O::sub(m.pyz, O::mul(t.uy, t.uz));
-    return t;
-}
-
-// Ed_a = 3 tau u_a^2 (du_a/dx_a) for the three axes from the differences gx, gy, gz.
-template <class V>
-__device__ __forceinline__ void galilean_correction(Stress<V>& t, V om, V gx, V gy, V gz) {
-    using O = VO<V>;
-    const V tp3 = O::mul(O::k(3.0f), O::rcp(om));
-    t.pxx = O::sub(t.pxx, O::mul(O::mul(O::mul(tp3, t.ux), t.ux), gx));
-    t.pyy = O::sub(t.pyy, O::mul(O::mul(O::mul(tp3, t.uy), t.uy), gy));
-    t.pzz = O::sub(t.pzz, O::mul(O::mul(O::mul(tp3, t.uz), t.uz), gz));
-}
-
-template <int ST, bool GAL, class V>
-__device__ __forceinline__ void regularised_out(void* fout, uint32_t NP, int32_t n, V dr, V om, const Stress<V>& t) {
-    using O = VO<V>;
-    const V trp = O::mul(O::add(O::add(t.pxx, t.pyy), t.pzz), O::k(1.0f / 3.0f));
-    const V s = O::mul(O::k(4.5f), O::sub(O::k(1.0f), om));         // 4.5 (1 - om)
-    const V A = O::sub(O::fma(O::k(-1.5f), t.usq, dr), O::mul(s, trp));
-    const V hx = O::mul(O::k(4.5f), t.ux), hy = O::mul(O::k(4.5f), t.uy), hz = O::mul(O::k(4.5f), t.uz);
-    const V s2 = O::add(s, s), hx2 = O::add(hx, hx), hy2 = O::add(hy, hy);
-    store_regularised<ST, GAL, V>(fout, NP, n, A, t.ux, t.uy, t.uz, O::fma(hx, t.ux, O::mul(s, t.pxx)),
-                                  O::fma(hy, t.uy, O::mul(s, t.pyy)), O::fma(hz, t.uz, O::mul(s, t.pzz)),
-                                  O::fma(hx2, t.uy, O::mul(s2, t.pxy)), O::fma(hx2, t.uz, O::mul(s2, t.pxz)),
-                                  O::fma(hy2, t.uz, O::mul(s2, t.pyz)));
+    const float tr = sxy + mzz, ca = tr + mxy2, cb = tr - mxy2, cg = mxz2 + myz2, cd = mxz2 - myz2;
+    store_pair<ST, 19>(fout, NP, n, A, ca + cg, (3.0f * SC) * (u7 + uz) + h19);
+    store_pair<ST, 21>(fout, NP, n, A, ca - cg, (3.0f * SC) * (u7 - uz) + h21);
+    store_pair<ST, 23>(fout, NP, n, A, cb + cd, (3.0f * SC) * (u9 + uz) + h23);
+    store_pair<ST, 25>(fout, NP, n, A, cb - cd, (3.0f * SC) * (uz - u9) + h25);
 }
 
 // ---- 1. boundary-link kernel and clock ----------------------------------------------------------------------------
@@ -601,7 +513,7 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
     }
 
     // the 27 pulls (TRT and the body-force path use the populations themselves after the moments)
-    Moments<float> m;
+    Moments m;
     float fk[Q];
     Unroll<0, Q>::run([&](auto ic) {
         constexpr int I = decltype(ic)::value;
@@ -611,44 +523,6 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
 
     const bool inlet_cell = om_signed < 0.0f;
     const float om = fabsf(om_signed);
-    if constexpr (MODEL == CS_MODEL_REGULARISED && !FORCE) {
-        if (!inlet_cell) {
-            // the regularised step without a body force: the same operations as the node-pair kernel's
-            Stress<float> t = regularised_stress(m);
-            if (d.sigma < 1.0f) {
-                // hybrid regularisation (lbm.py:224-229): G[a][b] = du_b/dx_a from the previous step's velocity
-                float gr[3][3];
-                const float u0[3] = {upx, upy, upz};
-#pragma unroll
-                for (int ax = 0; ax < 3; ++ax) {
-                    const int km = 1 + 2 * ax, kp = 2 + 2 * ax;
-#pragma unroll
-                    for (int c = 0; c < 3; ++c)
-                        gr[ax][c] = ddx_g(lk[km], lk[kp], __ldg(grad_src(d, vin, km, c, lk[km])),
-                                          __ldg(grad_src(d, vin, kp, c, lk[kp])), u0[c], N);
-                }
-                const float sg = d.sigma, k = (1.0f - sg) / (3.0f * om);
-                t.pxx = sg * t.pxx - k * (2.0f * gr[0][0]);
-                t.pyy = sg * t.pyy - k * (2.0f * gr[1][1]);
-                t.pzz = sg * t.pzz - k * (2.0f * gr[2][2]);
-                t.pxy = sg * t.pxy - k * (gr[0][1] + gr[1][0]);
-                t.pxz = sg * t.pxz - k * (gr[0][2] + gr[2][0]);
-                t.pyz = sg * t.pyz - k * (gr[1][2] + gr[2][1]);
-            }
-            if (GAL)
-                galilean_correction(t, om, ddx_g(lk[1], lk[2], g[0], g[1], upx, N),
-                                    ddx_g(lk[3], lk[4], g[2], g[3], upy, N), ddx_g(lk[5], lk[6], g[4], g[5], upz, N));
-            regularised_out<ST, GAL, float>(fout, NP, n, m.dr, om, t);
-            vout[n] = t.ux;
-            vout[N + n] = t.uy;
-            vout[2 * N + n] = t.uz;
-            d.rho[n] = m.dr;
-            ux_o = t.ux;
-            uy_o = t.uy;
-            uz_o = t.uz;
-            return;
-        }
-    }
     // without a body force (FORCE false) every force term folds away at compile time
     const float Fx = FORCE ? d.force[0] * dv : 0.0f, Fy = FORCE ? d.force[1] * dv : 0.0f;
     const float Fz = FORCE ? d.force[2] * dv : 0.0f;
@@ -689,8 +563,7 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
 
     const Cubic cu3(ux, uy, uz);
     if constexpr (MODEL == CS_MODEL_REGULARISED) {
-        // (without a body force the regularised step returned above)
-        float pxx = 0.f, pyy = 0.f, pzz = 0.f, pxy = 0.f, pxz = 0.f, pyz = 0.f;
+        float pxx, pyy, pzz, pxy, pxz, pyz;
         if constexpr (FORCE) {
             // with a body force, P link by link as the reference sums it (lbm.py:220-223): a slowly forced steady
             // state (Poiseuille at tau ~ 0.505, forces ~1e-7) keeps the FP32 rounding of this order
@@ -707,6 +580,10 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
                 if (x && z) pxz += float(x * z) * sv;
                 if (y && z) pyz += float(y * z) * sv;
             });
+        } else {
+            const float d3 = dr * (1.0f / 3.0f);
+            pxx = m.pxx - d3 - ux * ux, pyy = m.pyy - d3 - uy * uy, pzz = m.pzz - d3 - uz * uz;
+            pxy = m.pxy - ux * uy, pxz = m.pxz - ux * uz, pyz = m.pyz - uy * uz;
         }
         if (d.sigma < 1.0f) {
             // hybrid regularisation (lbm.py:224-229): G[a][b] = du_b/dx_a from the previous step's velocity
@@ -763,6 +640,14 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
             uz_o = uz;
             return;
         }
+        // without a force: f_out = feq + (1 - om) fneq + (1 - om/2) src (lbm.py:236-240) regrouped as
+        // w (A + E +- O), each pair's terms evaluated once
+        const float A = dr - 1.5f * usq - 4.5f * k_ne * trp;
+        const float s = 4.5f * k_ne;
+        const float hx = 4.5f * ux, hy = 4.5f * uy;
+        store_regularised<ST, GAL>(fout, NP, n, A, ux, uy, uz, fmaf(hx, ux, s * pxx), fmaf(hy, uy, s * pyy),
+                                   fmaf(4.5f * uz, uz, s * pzz), fmaf(2.0f * hx, uy, 2.0f * s * pxy),
+                                   fmaf(2.0f * hx, uz, 2.0f * s * pxz), fmaf(2.0f * hy, uz, 2.0f * s * pyz));
     } else {
         // TRT + Guo forcing (lbm.py:241-255)
         const float om_m = 1.0f / (0.5f + d.magic / (1.0f / om - 0.5f));
@@ -864,166 +749,6 @@ __global__ void __launch_bounds__(DENSE_BLOCK, DENSE_MIN_BLOCKS) k_bulk_dense(co
     bulk_body<ST, CS_MODEL_REGULARISED, GAL, false>(d, a, blockIdx.x);
 }
 
-// ---- 2b. node-pair bulk kernel --------------------------------------------------------------------------------------
-// The regularised step without a body force (every open vessel and the benchmark workloads), two consecutive nodes
-// per thread. When both nodes are regular in the same segment of the compressed connectivity (their 27 sources are
-// fluid nodes n + delta_i and n + 1 + delta_i), they share one decode of the segment row and one address per link,
-// their arithmetic runs as packed FP32x2 instructions (one instruction for both nodes), and every output is one
-// aligned store of both nodes' values (64-bit in FP32, 32-bit in the 16-bit formats). Any other pair (a node with a
-// boundary link, an inlet cell, a segment boundary between the two, an odd last node) is updated node by node by
-// node_update. Both paths evaluate the same explicitly rounded operations, so a node's result does not depend on
-// which path took it. Needs an even population row length (the pair stores are aligned) and no outlet coupling
-// (the flux partition is per block of `block` nodes); the host selects it only then.
-constexpr int PAIR_BLOCK = 128;
-#ifndef CS_PAIR_MIN_BLOCKS
-#define CS_PAIR_MIN_BLOCKS 5
-#endif
-#ifndef CS_PAIR_STRIDE
-#define CS_PAIR_STRIDE 32
-#endif
-constexpr int PAIR_MIN_BLOCKS = CS_PAIR_MIN_BLOCKS;
-// Distance between a thread's two nodes: 32 (a warp takes 64 consecutive nodes, lane t nodes t and t + 32, so every
-// load and store of the warp covers 32 consecutive elements) or 1 (nodes 2t and 2t + 1: paired 64/32-bit stores,
-// but every load instruction touches each sector twice).
-constexpr int PAIR_STRIDE = CS_PAIR_STRIDE;
-static_assert(PAIR_STRIDE == 1 || PAIR_STRIDE == 32, "pair stride");
-
-// Two populations at idx and idx + S, scaled to f - w (float2: the pair's two nodes).
-template <int ST, int S> struct Pop2;
-template <int S> struct Pop2<CS_STORE_F32, S> {
-    static __device__ __forceinline__ float2 ld(const void* b, uint32_t idx, float) {
-        const float* p = static_cast<const float*>(b) + idx;
-        return make_float2(__ldg(p), __ldg(p + S));
-    }
-    static __device__ __forceinline__ void st(void* b, uint32_t idx, float2 g) {
-        float* p = static_cast<float*>(b) + idx;
-        if constexpr (S == 1) {
-            *reinterpret_cast<float2*>(p) = g;
-        } else {
-            p[0] = g.x;
-            p[S] = g.y;
-        }
-    }
-};
-template <int S> struct Pop2<CS_STORE_F16, S> {
-    static __device__ __forceinline__ float2 ld(const void* b, uint32_t idx, float w) {
-        const __half* p = static_cast<const __half*>(b) + idx;
-        return VO<float2>::mul(make_float2(__half2float(__ldg(p)), __half2float(__ldg(p + S))),
-                               VO<float2>::k(w * (1.0f / 1024.0f)));
-    }
-    static __device__ __forceinline__ void st(void* b, uint32_t idx, float2 g) {
-        __half* p = static_cast<__half*>(b) + idx;
-        if constexpr (S == 1) {
-            *reinterpret_cast<__half2*>(p) = __float22half2_rn(g);
-        } else {
-            p[0] = __float2half_rn(g.x);
-            p[S] = __float2half_rn(g.y);
-        }
-    }
-};
-template <int S> struct Pop2<CS_STORE_BF16, S> {
-    static __device__ __forceinline__ float2 ld(const void* b, uint32_t idx, float w) {
-        const __nv_bfloat16* p = static_cast<const __nv_bfloat16*>(b) + idx;
-        return VO<float2>::mul(make_float2(__bfloat162float(__ldg(p)), __bfloat162float(__ldg(p + S))),
-                               VO<float2>::k(w * (1.0f / 1024.0f)));
-    }
-    static __device__ __forceinline__ void st(void* b, uint32_t idx, float2 g) {
-        __nv_bfloat16* p = static_cast<__nv_bfloat16*>(b) + idx;
-        if constexpr (S == 1) {
-            *reinterpret_cast<__nv_bfloat162*>(p) = __float22bfloat162_rn(g);
-        } else {
-            p[0] = __float2bfloat16_rn(g.x);
-            p[S] = __float2bfloat16_rn(g.y);
-        }
-    }
-};
-
-template <int ST>
-__device__ __forceinline__ void PopV<ST, float2>::st_scaled(void* b, uint32_t idx, float2 g) {
-    Pop2<ST, PAIR_STRIDE>::st(b, idx, g);
-}
-
-// Nodes n and n + PAIR_STRIDE, both regular in segment `code`.
-template <int ST, bool GAL>
-__device__ __forceinline__ void pair_update(const cs_step_desc& d, const int a, const int32_t n, const int32_t code) {
-    using O = VO<float2>;
-    constexpr int S = PAIR_STRIDE;
-    const int32_t N = int32_t(d.n);
-    const uint32_t NP = uint32_t(d.npad);
-    const void* fin = d.f[a];
-    void* fout = d.f[1 - a];
-    const float* vin = d.vel[a];
-    float* vout = d.vel[1 - a];
-    // static tables first: the segment row (seven 128-bit loads, shared by the warp's nodes of the segment), omega
-    int32_t lk[Q];
-    const int4* sd = reinterpret_cast<const int4*>(d.segdelta + int64_t(code) * CS_SEG_STRIDE);
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-        const int4 v = __ldg(sd + k);
-        lk[4 * k] = n + v.x;
-        if (4 * k + 1 < Q) lk[4 * k + 1] = n + v.y;
-        if (4 * k + 2 < Q) lk[4 * k + 2] = n + v.z;
-        if (4 * k + 3 < Q) lk[4 * k + 3] = n + v.w;
-    }
-    const float2 om = make_float2(__ldg(d.om + n), __ldg(d.om + n + S));
-    grid_dependency_wait();
-    // the six axis neighbours' previous velocity (fluid for a regular node) for the Galilean differences
-    float2 g[6];
-    if (GAL) {
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const float* p = vin + int64_t(k / 2) * N + lk[1 + k];
-            g[k] = make_float2(__ldg(p), __ldg(p + S));
-        }
-    }
-    float2 fk[Q];
-    Unroll<0, Q>::run([&](auto ic) {
-        constexpr int I = decltype(ic)::value;
-        fk[I] = Pop2<ST, S>::ld(fin, uint32_t(I) * NP + uint32_t(lk[I]), wgt(I));
-    });
-    Moments<float2> m;
-    moments27(fk, m);
-    Stress<float2> t = regularised_stress(m);
-    if (GAL) {
-        const float2 h = O::k(0.5f);
-        galilean_correction(t, om, O::mul(h, O::sub(g[1], g[0])), O::mul(h, O::sub(g[3], g[2])),
-                            O::mul(h, O::sub(g[5], g[4])));
-    }
-    regularised_out<ST, GAL, float2>(fout, NP, n, m.dr, om, t);
-    vout[n] = t.ux.x;
-    vout[n + S] = t.ux.y;
-    vout[N + n] = t.uy.x;
-    vout[N + n + S] = t.uy.y;
-    vout[2 * N + n] = t.uz.x;
-    vout[2 * N + n + S] = t.uz.y;
-    d.rho[n] = m.dr.x;
-    d.rho[n + S] = m.dr.y;
-}
-
-template <int ST, bool GAL>
-__global__ void __launch_bounds__(PAIR_BLOCK, PAIR_MIN_BLOCKS) k_bulk_pair(const cs_step_desc d, const int a) {
-    constexpr int S = PAIR_STRIDE;
-    const int32_t t = int32_t(blockIdx.x) * int32_t(blockDim.x) + int32_t(threadIdx.x);
-    // stride 1: nodes 2t, 2t + 1; stride 32: warp w's 64 nodes from 64 w, lane l takes l and l + 32
-    const int32_t n = S == 1 ? 2 * t : 64 * (t >> 5) + (t & 31);
-    if (n < d.n) {
-        int32_t c0 = -1, c1 = -2;
-        if (n + S < d.n) {
-            c0 = __ldg(d.lcode + n);
-            c1 = __ldg(d.lcode + n + S);
-        }
-        if (c0 >= 0 && c0 == c1) {
-            pair_update<ST, GAL>(d, a, n, c0);
-        } else {
-            float ux, uy, uz;
-            node_update<ST, CS_MODEL_REGULARISED, GAL, false>(d, a, n, ux, uy, uz);
-            if (n + S < d.n) node_update<ST, CS_MODEL_REGULARISED, GAL, false>(d, a, n + S, ux, uy, uz);
-        }
-    }
-    grid_dependency_wait();
-    launch_dependents();
-}
-
 // ---- 3. outlet resistances ----------------------------------------------------------------------------------------
 constexpr int BC_THREADS = 256;
 
@@ -1082,18 +807,8 @@ StepFn pick_force(int model, int gal, bool force, int block) {
     return force ? k_bulk<ST, CS_MODEL_TRT, false, true> : k_bulk<ST, CS_MODEL_TRT, false, false>;
 }
 
-// The node-pair kernel applies: the regularised step without a body force, hybrid blend or outlet coupling, blocks
-// of at most PAIR_BLOCK threads and an even population row length.
-bool use_pairs(const cs_step_desc& d) {
-    const bool force = d.force[0] != 0.0f || d.force[1] != 0.0f || d.force[2] != 0.0f;
-    const int block = d.block ? d.block : MAX_BLOCK;
-    return d.model == CS_MODEL_REGULARISED && !force && d.sigma >= 1.0f && d.n_open == 0 && block <= PAIR_BLOCK &&
-           (PAIR_STRIDE != 1 || d.npad % 2 == 0);
-}
-
 template <int ST>
 StepFn pick_model(const cs_step_desc& d) {
-    if (use_pairs(d)) return d.gal ? k_bulk_pair<ST, true> : k_bulk_pair<ST, false>;
     const bool force = d.force[0] != 0.0f || d.force[1] != 0.0f || d.force[2] != 0.0f;
     return pick_force<ST>(d.model, d.gal, force, d.block ? d.block : MAX_BLOCK);
 }
@@ -1117,9 +832,8 @@ StepFn pick_boundary(const cs_step_desc& d) {
 int validate(const cs_step_desc* d) {
     if (!d) return fail(CS_ERR_ARG, "cs_step: null descriptor");
     if (d->n < 0 || d->n >= (int64_t(1) << 30)) return fail(CS_ERR_SIZE, "cs_step: n = %lld", (long long)d->n);
-    if (d->gmax < 0 || d->npad < d->n + d->gmax || int64_t(Q) * d->npad >= (int64_t(1) << 31))
-        return fail(CS_ERR_SIZE, "cs_step: npad %lld must be at least n + gmax with 27 * npad < 2^31",
-                    (long long)d->npad);
+    if (d->gmax < 0 || d->npad != d->n + d->gmax || int64_t(Q) * d->npad >= (int64_t(1) << 31))
+        return fail(CS_ERR_SIZE, "cs_step: npad %lld must be n + gmax with 27 * npad < 2^31", (long long)d->npad);
     if (d->gblock[0] != 0) return fail(CS_ERR_ARG, "cs_step: gblock[0] = %d", d->gblock[0]);
     for (int i = 0; i < Q; ++i) {
         const int64_t w = int64_t(d->gblock[i + 1]) - d->gblock[i];
@@ -1165,8 +879,7 @@ int launch_pdl(StepFn fn, dim3 grid, dim3 block, cudaStream_t st, const cs_step_
 
 int launch_steps(const cs_step_desc* d, int a, int steps, cudaStream_t st) {
     const int block = d->block ? d->block : MAX_BLOCK;
-    const int64_t per_block = use_pairs(*d) ? 2 * int64_t(block) : int64_t(block);      // nodes per bulk block
-    const unsigned grid = unsigned(d->n > 0 ? ceil_div(d->n, per_block) : 0);
+    const unsigned grid = unsigned(d->n > 0 ? ceil_div(d->n, block) : 0);
     const dim3 bgrid(unsigned(boundary_items(*d)));
     StepFn bulk = pick_bulk(*d);
     StepFn bound = pick_boundary(*d);

@@ -245,8 +245,7 @@ class Solver:
                 check(lib.cs_links_count(_ptr(nbr), N, _ptr(scratch), ghosts, sp))
                 self.ghosts = [int(x) for x in ghosts]
                 self.gmax = max(self.ghosts) if N else 0
-                # rows padded to a multiple of 8 slots: the node-pair kernel's paired stores need an even length
-                self.npad = -(-(N + self.gmax) // 8) * 8
+                self.npad = N + self.gmax
                 gcols = max(1, self.gmax)
                 self.links = torch.empty((Q, N), dtype=torch.int32, device=dev)
                 self.gnode = torch.full((Q, gcols), -1, dtype=torch.int32, device=dev)
