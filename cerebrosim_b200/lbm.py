@@ -453,6 +453,53 @@ class Solver:
             p = rho.cpu().numpy()
         return p / 3.0, u
 
+    # --- checkpoint / resume (the reference saves outputs only and restarts whole runs, README.md:144)
+    _STATE = ("rho", "p_out", "p_out64", "tick", "drv", "coef", "om")
+
+    def checkpoint(self):
+        """The solver's evolving state as host tensors: the current populations (in their storage format, ghost
+        slots included), the current velocity, density, clock, drive coefficients, outlet pressures and relaxation
+        rates, and the step count. `restore` on a solver built from the same lattice and settings continues the run
+        bit for bit."""
+        self.stream.synchronize()
+        st = {k: getattr(self, k).detach().cpu().clone() for k in self._STATE}
+        # the two-slot clock: the restored solver reads buffer 0, so both slots carry the count of the next step
+        st["tick"] = self.tick[self.cur].detach().cpu().repeat(2)
+        st.update({"f": self.f[self.cur].detach().cpu().clone(), "vel": self.vel[self.cur].detach().cpu().clone(),
+                   "steps": int(self.steps), "N": int(self.N), "storage": self.storage, "order": self.order,
+                   "drive": (int(self.nh), int(self.period), int(self.ramp)), "force": tuple(self.force)})
+        return st
+
+    def restore(self, st):
+        """Load a `checkpoint` taken on a solver of the same lattice, storage format and node order."""
+        if (st["N"], st["storage"], st["order"]) != (self.N, self.storage, self.order):
+            raise ValueError(f"checkpoint of {st['N']} nodes, {st['storage']}, order {st['order']}: this solver has "
+                             f"{self.N}, {self.storage}, order {self.order}")
+        if tuple(st["f"].shape) != tuple(self.f[0].shape):
+            raise ValueError("checkpoint populations have another shape (different ghost slots)")
+        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+            self.cur = 0
+            self.f[0].copy_(st["f"].to(self.dev))
+            self.vel[0].copy_(st["vel"].to(self.dev))
+            for k in self._STATE:
+                if k == "coef":
+                    self.coef = st["coef"].to(self.dev)
+                else:
+                    getattr(self, k).copy_(st[k].to(self.dev))
+        self.nh, self.period, self.ramp = st["drive"]
+        self.force = tuple(st["force"])
+        self.steps = int(st["steps"])
+        self._drop_graphs()
+        self.stream.synchronize()
+
+    def save(self, path):
+        """Write a checkpoint to `path` (torch.save)."""
+        torch.save(self.checkpoint(), path)
+
+    def load(self, path):
+        """Restore the checkpoint written by `save`."""
+        self.restore(torch.load(path, weights_only=False))
+
     def ok(self):
         """All densities finite (lbm.py:454-455)."""
         self.stream.synchronize()

@@ -117,6 +117,19 @@ class ArterySolver(Solver):
         d.pref, d.alpha = self.pref, self.alpha
         d.beat_acc = self._beat_acc.data_ptr()
 
+    def checkpoint(self):
+        """lbm.Solver.checkpoint plus the coupling's state: last flows, FP64 outlet pressures, beat sums."""
+        st = super().checkpoint()
+        st.update({"q_last": self._qlast.cpu().clone(), "beat_acc": self._beat_acc.cpu().clone()})
+        return st
+
+    def restore(self, st):
+        super().restore(st)
+        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+            self._qlast.copy_(st["q_last"].to(self.dev))
+            self._beat_acc.copy_(st["beat_acc"].to(self.dev))
+        self.stream.synchronize()
+
     def beat_means(self, reset=True):
         """Means of the open ends' pressures p_out (lattice units) and flows Qlast over the steps since the last
         reset, accumulated on the device in FP64 by every step's k_bc -> (p (n_open,), Q (n_open,), steps). The
