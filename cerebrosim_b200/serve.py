@@ -85,11 +85,14 @@ class Server:
 
     Divergence: at every beat end (before on_beat) a request's densities are checked for non-finite values
     (simulate.py:321-322 raises there); a request that has diverged is evicted at once — its steps stop, its slot and
-    budget are released, and it ends with ok = False and `evicted` = the beat — while the others go on unchanged."""
+    budget are released, and it ends with ok = False and `evicted` = the beat — while the others go on unchanged.
+
+    log(record): called at every beat end with a JSON-ready dict — request id, beat, device time (s), the beat's
+    latency (s), nodes and the request's update rate over the beat (MLUPS) — for a per-beat metrics stream."""
 
     def __init__(self, budget_bytes=150e9, storage="bf16", steps_per_beat=8000, chunk=1000, graph_chunk=200,
                  max_active=64, block=128, ahead=2, keep_fields=True, device=None, builder=default_builder,
-                 order="c", on_beat=None, schedule="fused"):
+                 order="c", on_beat=None, schedule="fused", log=None):
         if steps_per_beat % chunk or chunk % 2 or graph_chunk % 2:
             raise ValueError("chunk must divide steps_per_beat; chunk and graph_chunk must be even")
         self.budget = float(budget_bytes)
@@ -105,6 +108,7 @@ class Server:
         self.builder = builder
         self.order = order
         self.on_beat = on_beat
+        self.log = log
         self.schedule = schedule
         self.trace = []         # (seconds, active requests, reserved bytes) after each admission
 
@@ -165,6 +169,10 @@ class Server:
                 continue
             if steps % self.steps_per_beat == 0:
                 r.beat_end.append(t)
+                if self.log is not None:
+                    lat = r.beat_latencies()[-1]
+                    self.log({"request": r.id, "beat": steps // self.steps_per_beat, "t_s": t, "latency_s": lat,
+                              "nodes": r.N, "mlups": r.N * self.steps_per_beat / max(lat, 1e-12) / 1e6})
                 if steps < r.steps_total:
                     beat = steps // self.steps_per_beat
                     if not self._finite(r):

@@ -63,8 +63,13 @@ def test_served_matches_dedicated_solver(schedule):
 
 
 def test_admission_by_budget():
-    sv = server("bf16", budget_bytes=2.5 * serve.BYTES_PER_NODE["bf16"] * 60e3)
+    records = []
+    sv = server("bf16", budget_bytes=2.5 * serve.BYTES_PER_NODE["bf16"] * 60e3, log=records.append)
     reqs = sv.serve(specs(), realtime=False)
+    # the per-beat metrics stream: one record per beat of every request, JSON-ready
+    import json
+    assert len(records) == sum(r.beats for r in reqs) and json.loads(json.dumps(records)) == records
+    assert all(x["latency_s"] > 0 and x["mlups"] > 0 for x in records)
     assert all(r.ok for r in reqs)
     assert all(used <= sv.budget for _, _, used in sv.trace)
     # not everything fitted at once: some request waited for memory to free up
