@@ -494,19 +494,26 @@ def main():
     torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_host = [time.perf_counter()]
     e0.record()
     s2 = lbm.Solver(host, nu_lu(), model="regularised", device=dev, storage=args.storage, **shape)
     configure(s2)
+    t_host.append(time.perf_counter())
     s2.run(args.steps)
+    s2.synchronize()
+    t_host.append(time.perf_counter())
     p_h, u_h = s2.fields()
     e1.record()
     torch.cuda.synchronize()
+    t_host.append(time.perf_counter())
     e2e_secs = max_over_ranks(e0.elapsed_time(e1) * 1e-3)
     d2h = p_h.nbytes + u_h.nbytes
     e2e = {"value": world * N * args.steps / e2e_secs / 1e6, "unit": "MLUPS",
            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
            "definition": "Solver(lat) from pinned host tables + run(K) in CUDA graphs + fields() readback, "
-                         "no L2 flush"}
+                         "no L2 flush",
+           "parts_ms": {"construct": (t_host[1] - t_host[0]) * 1e3, "run": (t_host[2] - t_host[1]) * 1e3,
+                        "fields": (t_host[3] - t_host[2]) * 1e3}}
 
     # the batched sweep and the served stream: every rank runs its share (the same collective calls on every rank)
     extra = {}
