@@ -68,14 +68,19 @@ def measured_peak():
 
 
 def profiled_traffic(storage):
-    """DRAM bytes per node update of the step kernel from the committed ncu summary (None if not captured)."""
+    """DRAM bytes per node update of both step kernels, and the build they were captured on, from the committed ncu
+    summary -> (bytes, source) or (None, None) when no capture exists for this storage format."""
     p = os.path.join(ROOT, "profiles", f"step_{storage}_open_pipe_R24_L192.md")
     if not os.path.exists(p):
-        return None
+        return None, None
+    val, build = None, "?"
     for line in open(p):
         if line.startswith("dram_bytes_per_node_update:"):
-            return float(line.split(":")[1])
-    return None
+            val = float(line.split(":")[1])
+        if line.startswith("Build: commit"):
+            build = line.split()[2]
+    return val, f"ncu dram__bytes_read.sum + dram__bytes_write.sum of k_boundary + k_bulk_dense, one capture on " \
+                 f"commit {build} (profiles/step_{storage}_open_pipe_R24_L192.md)"
 
 
 class Clocks:
@@ -478,7 +483,7 @@ def main():
     peak, peak_kind = measured_peak()
     bplu = BPLU[args.storage]
     achieved = bplu * N / mean_step / 1e9
-    tr = profiled_traffic(args.storage)
+    tr, tr_source = profiled_traffic(args.storage)
 
     # end to end through the public API: host tables (pinned) -> Solver -> run(K) in graphs -> fields()
     host = {k: (torch.from_numpy(np.ascontiguousarray(lat[k])).pin_memory() if k in ("nbr", "q", "uin") else lat[k])
@@ -537,7 +542,8 @@ def main():
                 "hbm_gbs": achieved,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_kind": peak_kind,
-                             "traffic": tr * N if tr else None, "bytes_per_update": bplu,
+                             "traffic": tr * N if tr else None, "traffic_source": tr_source,
+                             "bytes_per_update": bplu,
                              "kernel": "one step = k_boundary + the bulk kernel (k_bulk_pair: two nodes per "
                                        "thread), timed together"},
                 "back_to_back": {"ms_per_step": b2b * 1e3, "value": world * N / b2b / 1e6, "unit": "MLUPS",
