@@ -47,8 +47,7 @@ class StepDesc(ctypes.Structure):
                 ("q_part", ctypes.c_void_p), ("fb_list", ctypes.c_void_p), ("n_fb", ctypes.c_int32),
                 ("q_last", ctypes.c_void_p), ("p_out64", ctypes.c_void_p),
                 ("r_out", ctypes.c_void_p), ("pref", ctypes.c_double), ("alpha", ctypes.c_double),
-                ("gblock", ctypes.c_int32 * 28), ("beat_acc", ctypes.c_void_p),
-                ("gbin", ctypes.c_void_p)]
+                ("gblock", ctypes.c_int32 * 28), ("beat_acc", ctypes.c_void_p)]
 
 
 class BatchDesc(ctypes.Structure):
@@ -96,7 +95,6 @@ SIGNATURES = {
     "cs_last_error": (_I32, [ctypes.c_char_p, _I32]),
     "cs_version": (ctypes.c_char_p, []),
     "cs_abi_sizeof": (_SZ, [_I32]),
-    "cs_gbin_refresh": (_I32, [ctypes.POINTER(StepDesc), _I32, _P]),
 }
 
 _lib = None

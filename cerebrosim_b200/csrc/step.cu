@@ -82,29 +82,6 @@ template <> struct Pop<CS_STORE_BF16> {
     }
 };
 
-// Raw storage bits of one population (Bits) and the value Pop<ST>::ld makes of them; a boundary slot's record of the
-// two populations its rule reads at its node is a pair of them (Bits2).
-template <int ST> struct Raw;
-template <> struct Raw<CS_STORE_F32> {
-    using Bits = uint32_t;
-    using Bits2 = uint2;
-    static __device__ __forceinline__ float val(Bits b, float) { return __uint_as_float(b); }
-};
-template <> struct Raw<CS_STORE_F16> {
-    using Bits = unsigned short;
-    using Bits2 = ushort2;
-    static __device__ __forceinline__ float val(Bits b, float w) {
-        return __half2float(__ushort_as_half(b)) * (w * (1.0f / 1024.0f));
-    }
-};
-template <> struct Raw<CS_STORE_BF16> {
-    using Bits = unsigned short;
-    using Bits2 = ushort2;
-    static __device__ __forceinline__ float val(Bits b, float w) {
-        return __bfloat162float(__ushort_as_bfloat16(b)) * (w * (1.0f / 1024.0f));
-    }
-};
-
 // ---- helpers ------------------------------------------------------------------------------------------------------
 __device__ __forceinline__ float drive_value(const cs_step_desc& d, int t) {
     // lbm.py:95-100, float32
@@ -386,21 +363,13 @@ __device__ __forceinline__ void boundary_body(const cs_step_desc& d, const int a
     const bool is_wall = info >= CS_WALL, is_inlet = info == CS_INLET;
     float fo = 0.0f, f2 = 0.0f, e0 = 0.0f, e1 = 0.0f, e2 = 0.0f, pk = 0.0f;
     if (live_node) {
-        // the node's populations opp(i) and i: from the slot's record (one coalesced load), which the last step's
-        // bulk kernel copied from the same buffer, or scattered from the populations themselves
-        typename Raw<ST>::Bits2 rec{};
-        if (d.gbin) {
-            rec = __ldg(static_cast<const typename Raw<ST>::Bits2*>(d.gbin) + slot);
-            fo = Raw<ST>::val(rec.x, wo);
-        } else {
-            fo = Pop<ST>::ld(fin, uint32_t(io) * NP + nn, wo);
-        }
+        fo = Pop<ST>::ld(fin, uint32_t(io) * NP + nn, wo);
         if (is_wall) {
             if (d.bouzidi) {
                 if (qslot < 0.5f) {
                     if (info >= 0) f2 = Pop<ST>::ld(fin, uint32_t(io) * NP + uint32_t(info), wo);
                 } else {
-                    f2 = d.gbin ? Raw<ST>::val(rec.y, w) : Pop<ST>::ld(fin, uint32_t(i) * NP + nn, w);
+                    f2 = Pop<ST>::ld(fin, uint32_t(i) * NP + nn, w);
                 }
             }
         } else if (is_inlet) {
@@ -711,33 +680,6 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
     uz_o = uz;
 }
 
-// After its update, a node with boundary links copies, for each of them, the two populations the link's rule will
-// read at this node in the next step — its new populations opp(i) and i — into the link's slot record (d.gbin). The
-// boundary kernel then reads one coalesced record per link instead of two scattered populations; the copy reads
-// rows of consecutive nodes that this block has just written (coherent loads: L2, not the read-only path).
-template <int ST>
-__device__ __forceinline__ void copy_boundary_inputs(const cs_step_desc& d, const int a, const int32_t n) {
-    const int32_t code = __ldg(d.lcode + n);
-    if (code >= 0) return;                                  // every source is a fluid node: no boundary link
-    using Bits = typename Raw<ST>::Bits;
-    using Bits2 = typename Raw<ST>::Bits2;
-    const int32_t* ir = d.irr + (-1 - code);
-    const Bits* out = static_cast<const Bits*>(d.f[1 - a]);
-    Bits2* bin = static_cast<Bits2*>(d.gbin);
-    const uint32_t NP = uint32_t(d.npad);
-    const int32_t N = int32_t(d.n);
-#pragma unroll
-    for (int i = 1; i < Q; ++i) {
-        const int32_t s = __ldg(ir + int64_t(i) * d.n_irr);
-        if (s >= N) {
-            Bits2 r;
-            r.x = __ldcg(out + uint32_t(Lat::opp(i)) * NP + uint32_t(n));
-            r.y = __ldcg(out + uint32_t(i) * NP + uint32_t(n));
-            bin[int64_t(i) * d.gmax + (s - N)] = r;
-        }
-    }
-}
-
 // Block bx of a lattice's bulk grid (nodes bx * blockDim .. + blockDim - 1). Called by every thread of the block.
 template <int ST, int MODEL, bool GAL, bool FORCE>
 __device__ __forceinline__ void bulk_body(const cs_step_desc& d, const int a, const int bx) {
@@ -745,10 +687,7 @@ __device__ __forceinline__ void bulk_body(const cs_step_desc& d, const int a, co
     const int32_t n0 = int32_t(bx) * int32_t(blockDim.x);
     const int32_t n = n0 + int32_t(threadIdx.x);
     float ux = 0.f, uy = 0.f, uz = 0.f;
-    if (n < d.n) {
-        node_update<ST, MODEL, GAL, FORCE>(d, a, n, ux, uy, uz);
-        if (d.gbin) copy_boundary_inputs<ST>(d, a, n);
-    }
+    if (n < d.n) node_update<ST, MODEL, GAL, FORCE>(d, a, n, ux, uy, uz);
     grid_dependency_wait();      // (threads without a node) the flux accumulators were reset by the last step
     launch_dependents();
 
@@ -986,45 +925,6 @@ extern "C" int cs_flux_blocks(const int32_t* flux_idx, int64_t n_flux, int64_t n
     const int64_t nb = n > 0 ? ceil_div(n, block) : 1;
     k_flux_blocks<<<unsigned(ceil_div(nb + 1, 256)), 256, 0, as_stream(stream)>>>(flux_idx, n_flux, block, out, nb);
     CS_CHECK_LAUNCH("k_flux_blocks");
-    return CS_OK;
-}
-
-namespace cs {
-namespace {
-// Every boundary slot's record from buffer a's populations (after the populations were written from outside the
-// step, e.g. a restored checkpoint).
-template <int ST>
-__global__ void k_gbin_fill(const cs_step_desc d, const int a) {
-    using Bits = typename Raw<ST>::Bits;
-    using Bits2 = typename Raw<ST>::Bits2;
-    const int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-    if (t >= int64_t(Q) * d.gmax) return;
-    const int i = int(t / d.gmax);
-    const int32_t node = d.gnode[t];
-    if (node < 0) return;
-    const Bits* f = static_cast<const Bits*>(d.f[a]);
-    const uint32_t NP = uint32_t(d.npad);
-    Bits2 r;
-    r.x = f[uint32_t(Lat::opp(i)) * NP + uint32_t(node)];
-    r.y = f[uint32_t(i) * NP + uint32_t(node)];
-    static_cast<Bits2*>(d.gbin)[t] = r;
-}
-}  // namespace
-}  // namespace cs
-
-extern "C" int cs_gbin_refresh(const cs_step_desc* d, int32_t a, void* stream) {
-    int rc = validate(d);
-    if (rc != CS_OK) return rc;
-    if (a != 0 && a != 1) return fail(CS_ERR_ARG, "cs_gbin_refresh: a %d", a);
-    if (!d->gbin || d->gmax == 0) return CS_OK;
-    const unsigned grid = unsigned(ceil_div(int64_t(Q) * d->gmax, 256));
-    cudaStream_t st = as_stream(stream);
-    switch (d->storage) {
-        case CS_STORE_F16: k_gbin_fill<CS_STORE_F16><<<grid, 256, 0, st>>>(*d, a); break;
-        case CS_STORE_BF16: k_gbin_fill<CS_STORE_BF16><<<grid, 256, 0, st>>>(*d, a); break;
-        default: k_gbin_fill<CS_STORE_F32><<<grid, 256, 0, st>>>(*d, a); break;
-    }
-    CS_CHECK_LAUNCH("k_gbin_fill");
     return CS_OK;
 }
 

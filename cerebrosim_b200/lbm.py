@@ -272,9 +272,6 @@ class Solver:
                 del scratch
                 self.links = None                          # the full 27 x N table is not needed by the step
                 self.f = [torch.zeros((Q, self.npad), dtype=pop_dtype, device=dev) for _ in range(2)]
-                # per ghost slot, the raw pair of the node's populations opp(i), i that the slot's rule reads (kept by
-                # the bulk kernel; zero like the zero populations)
-                self.gbin = torch.zeros((Q, gcols, 2), dtype=pop_dtype, device=dev)
                 self.vel = [torch.zeros((3, N), dtype=torch.float32, device=dev) for _ in range(2)]
                 self.vels = [v.T for v in self.vel]
                 self.rho = torch.zeros(N, dtype=torch.float32, device=dev)
@@ -350,17 +347,8 @@ class Solver:
         d.tick, d.drive, d.coef = self.tick.data_ptr(), self.drv.data_ptr(), self.coef.data_ptr()
         d.nh, d.period, d.ramp = self.nh, self.period, self.ramp
         d.p_out64 = self.p_out64.data_ptr()
-        gb = getattr(self, "gbin", None)
-        d.gbin = gb.data_ptr() if gb is not None and self.gmax > 0 and gb.shape[1] >= self.gmax else None
         self._fill_desc(d)
         return d
-
-    def refresh_boundary(self):
-        """Recompute the boundary inputs the next step reads from the current populations: needed after writing
-        `f[cur]` from outside the step (the step keeps them itself)."""
-        with torch.cuda.device(self.dev):
-            check(_lib.load().cs_gbin_refresh(ctypes.byref(self._desc()), int(self.cur),
-                                              ctypes_void(self.stream.cuda_stream)))
 
     def _fill_desc(self, d):
         """Hook for subclasses that add the outlet-resistance coupling."""
@@ -502,7 +490,6 @@ class Solver:
         self.force = tuple(st["force"])
         self.steps = int(st["steps"])
         self._drop_graphs()
-        self.refresh_boundary()
         self.stream.synchronize()
 
     def save(self, path):

@@ -213,13 +213,6 @@ typedef struct cs_step_desc {
      * beat_acc[k] and q_last[k] to beat_acc[n_open + k] (FP64) and 1 to beat_acc[2 * n_open]; the caller zeroes
      * it at a beat's start and divides by the count at its end (the beat means of simulate.py:325-333). */
     double* beat_acc;
-    /* Boundary inputs (null: none): for each ghost slot (i, g), the raw stored values of the two populations its rule
-     * reads at its node, f[opp(i)][node] and f[i][node], as a pair in the storage format ([27][gmax] pairs, 8 bytes
-     * each in FP32, 4 in the 16-bit formats). Each step's bulk kernel writes them for the next step from the
-     * populations it has just stored; the boundary kernel reads one coalesced pair per link instead of two scattered
-     * populations. Zero-initialised with zero populations; after populations are written from outside the step, call
-     * cs_gbin_refresh. */
-    void* gbin;
 } cs_step_desc;
 
 /* Block partition of a sorted flux list for `block` threads per block: out[b] = first entry with
@@ -230,11 +223,6 @@ int cs_flux_blocks(const int32_t* flux_idx, int64_t n_flux, int64_t n, int32_t b
  * is the boundary-link kernel (one block per 256 boundary links of a direction, or a single block without any: it
  * also advances the clock), the bulk kernel and, when n_open > 0, the one-block k_bc kernel. */
 int cs_step(const cs_step_desc* d, int32_t a, int32_t steps, void* stream);
-
-/* Fill every ghost slot's boundary-input pair (cs_step_desc.gbin) from buffer a's populations: needed only after the
- * populations were written from outside the step (a restored checkpoint). No counterpart in the reference: the
- * records are this library's layout of what the reference's k_step reads at a wall node (lbm.py:163-173). */
-int cs_gbin_refresh(const cs_step_desc* d, int32_t a, void* stream);
 
 /* Check a descriptor (HOST struct) as cs_step does, without launching anything. */
 int cs_step_check(const cs_step_desc* d);

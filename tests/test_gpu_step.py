@@ -337,32 +337,3 @@ def test_checkpoint_resume_artery_solver(golden):
     assert np.array_equal(a.fields()[1], b.fields()[1])
     assert np.array_equal(a.Qlast.numpy(), b.Qlast.numpy()) and np.array_equal(a.p_out64.cpu().numpy(),
                                                                                 b.p_out64.cpu().numpy())
-
-
-@pytest.mark.parametrize("storage", ["f32", "bf16"])
-def test_boundary_input_records_change_no_bit(golden, storage):
-    """The boundary kernel reading each link's two populations from the per-slot records the bulk kernel keeps
-    (cs_step_desc.gbin) gives the same fields, bit for bit, as reading them from the populations, in every model
-    path: the regularised step, with a body force (the forced kernel), and TRT; and after populations written from
-    outside the step and refresh_boundary()."""
-    lg, _ = lattice_from_golden(golden, "stenosis70_D8")
-    for kw, force in ((dict(model="regularised"), None), (dict(model="regularised"), [0, 0, 1e-6]),
-                      (dict(model="trt"), None)):
-        out = []
-        for records in (True, False):
-            s = lbm.Solver(lg, 0.02, storage=storage, **kw)
-            if not records:
-                s.gbin = None
-            s.set_sponge(4, 0.6)
-            s.set_drive([0.02, 0.004, -0.003], period=300, ramp=150)
-            s.set_outlet_pressure([1e-4])
-            if force:
-                s.set_force(force)
-            s.run(301, chunk=100)
-            with torch.cuda.stream(s.stream):
-                s.f[s.cur].mul_(1.0001)                     # populations written from outside the step
-            if records:
-                s.refresh_boundary()
-            s.run(200, chunk=100)
-            out.append(s.fields())
-        assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1]), (kw, force)

@@ -101,7 +101,6 @@ def solver_on_noalloc_tables(lat, extra, stream):
     s.ghosts, s.gmax, s.npad = ghosts, gmax_cap, n + gmax_cap
     s.gnode, s.ginfo, s.gq = gnode, ginfo, gq
     s.f = [torch.zeros((27, s.npad), dtype=torch.float32, device=links.device) for _ in range(2)]
-    s.gbin = torch.zeros((27, max(1, gmax_cap), 2), dtype=torch.float32, device=links.device)
     s._drop_graphs()
     return s
 
