@@ -34,7 +34,7 @@ MAX_GROUPS = 64          # launch groups of CS_BATCH_GROUP instances: up to 4096
 # steps per CUDA graph of the fused schedule at most: each of its launches carries its group's 22 KB descriptor
 # table as kernel parameters, so a graph holds ~66 KB of parameters per step and group
 FUSED_GRAPH_MAX = 400
-SCHEDULES = ("fused", "by-instance", "concurrent:2", "concurrent:4")
+SCHEDULES = ("fused", "by-instance", "concurrent:2", "concurrent:4", "concurrent:8")
 
 
 class BatchSolver:
