@@ -35,7 +35,7 @@ def l2(a, b):
     return float(np.sqrt(((a.astype(np.float64) - b) ** 2).sum() / max((b.astype(np.float64) ** 2).sum(), 1e-300)))
 
 
-@pytest.mark.parametrize("schedule", ["fused", "by-instance"])
+@pytest.mark.parametrize("schedule", ["fused", "by-instance", "concurrent:2", "concurrent:4"])
 @pytest.mark.parametrize("storage", ["f32", "bf16"])
 def test_served_results_same_alone_and_in_the_mix(storage, schedule):
     sv = server(storage, max_active=3, schedule=schedule)
