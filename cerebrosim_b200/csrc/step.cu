@@ -472,36 +472,7 @@ __device__ __forceinline__ void store_pairs(void* fout, uint32_t NP, int32_t n, 
     });
 }
 
-// Staged pulls (the dense kernel): each thread copies its 27 populations into its own shared-memory slots with
-// cp.async and reads each back when the moments consume it, so the pulls in flight hold no registers. A 16-bit
-// population travels in the aligned 4-byte word that holds it (the row length is even, so the word lies inside the
-// buffer) and is read back from its half of the slot.
-#ifndef CS_STAGED_PULLS
-#define CS_STAGED_PULLS 1
-#endif
-constexpr int STAGE_BLOCK = 128;
-
-template <int ST>
-__device__ __forceinline__ void stage_pull(uint32_t* slot, const void* fin, uint32_t idx) {
-    const char* src = static_cast<const char*>(fin);
-    if constexpr (ST == CS_STORE_F32) src += size_t(idx) * 4u;
-    else src += (size_t(idx) * 2u) & ~size_t(3);
-    const unsigned dst = unsigned(__cvta_generic_to_shared(slot));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
-}
-
-template <int ST>
-__device__ __forceinline__ float staged_value(const uint32_t* slot, uint32_t idx, float w) {
-    if constexpr (ST == CS_STORE_F32) {
-        return __uint_as_float(*slot);
-    } else {
-        const unsigned short b = reinterpret_cast<const unsigned short*>(slot)[idx & 1u];
-        if constexpr (ST == CS_STORE_F16) return __half2float(__ushort_as_half(b)) * (w * (1.0f / 1024.0f));
-        else return __bfloat162float(__ushort_as_bfloat16(b)) * (w * (1.0f / 1024.0f));
-    }
-}
-
-template <int ST, int MODEL, bool GAL, bool FORCE, bool STAGED = false>
+template <int ST, int MODEL, bool GAL, bool FORCE>
 __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_t n, float& ux_o, float& uy_o,
                                             float& uz_o) {
     const int32_t N = int32_t(d.n);
@@ -544,23 +515,10 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
     // the 27 pulls (TRT and the body-force path use the populations themselves after the moments)
     Moments m;
     float fk[Q];
-    if constexpr (STAGED) {
-        __shared__ uint32_t s_pull[Q][STAGE_BLOCK];
-        Unroll<0, Q>::run([&](auto ic) {
-            constexpr int I = decltype(ic)::value;
-            stage_pull<ST>(&s_pull[I][threadIdx.x], fin, uint32_t(I) * NP + uint32_t(lk[I]));
-        });
-        asm volatile("cp.async.wait_all;" ::: "memory");
-        Unroll<0, Q>::run([&](auto ic) {
-            constexpr int I = decltype(ic)::value;
-            fk[I] = staged_value<ST>(&s_pull[I][threadIdx.x], uint32_t(I) * NP + uint32_t(lk[I]), wgt(I));
-        });
-    } else {
-        Unroll<0, Q>::run([&](auto ic) {
-            constexpr int I = decltype(ic)::value;
-            fk[I] = Pop<ST>::ld(fin, uint32_t(I) * NP + uint32_t(lk[I]), wgt(I));
-        });
-    }
+    Unroll<0, Q>::run([&](auto ic) {
+        constexpr int I = decltype(ic)::value;
+        fk[I] = Pop<ST>::ld(fin, uint32_t(I) * NP + uint32_t(lk[I]), wgt(I));
+    });
     moments27(fk, m);
 
     const bool inlet_cell = om_signed < 0.0f;
@@ -723,13 +681,13 @@ __device__ __forceinline__ void node_update(const cs_step_desc& d, int a, int32_
 }
 
 // Block bx of a lattice's bulk grid (nodes bx * blockDim .. + blockDim - 1). Called by every thread of the block.
-template <int ST, int MODEL, bool GAL, bool FORCE, bool STAGED = false>
+template <int ST, int MODEL, bool GAL, bool FORCE>
 __device__ __forceinline__ void bulk_body(const cs_step_desc& d, const int a, const int bx) {
     __shared__ float s_u[3][MAX_BLOCK];
     const int32_t n0 = int32_t(bx) * int32_t(blockDim.x);
     const int32_t n = n0 + int32_t(threadIdx.x);
     float ux = 0.f, uy = 0.f, uz = 0.f;
-    if (n < d.n) node_update<ST, MODEL, GAL, FORCE, STAGED>(d, a, n, ux, uy, uz);
+    if (n < d.n) node_update<ST, MODEL, GAL, FORCE>(d, a, n, ux, uy, uz);
     grid_dependency_wait();      // (threads without a node) the flux accumulators were reset by the last step
     launch_dependents();
 
@@ -784,17 +742,11 @@ __global__ void __launch_bounds__(MAX_BLOCK, MIN_BLOCKS) k_bulk(const cs_step_de
 // pulls' latency: 3-4 % faster steps from a cold L2 (the batched kernel, whose descriptor handling needs the
 // registers, keeps 64).
 constexpr int DENSE_BLOCK = 128;
-#ifndef CS_DENSE_MIN_BLOCKS
-#define CS_DENSE_MIN_BLOCKS 9
-#endif
-constexpr int DENSE_MIN_BLOCKS = CS_DENSE_MIN_BLOCKS;
-static_assert(DENSE_BLOCK <= STAGE_BLOCK, "staged pulls: one shared-memory slot row per thread");
+constexpr int DENSE_MIN_BLOCKS = 9;
 
-constexpr int BATCH_DENSE_MIN_BLOCKS = 9;
-
-template <int ST, bool GAL, bool STAGED>
+template <int ST, bool GAL>
 __global__ void __launch_bounds__(DENSE_BLOCK, DENSE_MIN_BLOCKS) k_bulk_dense(const cs_step_desc d, const int a) {
-    bulk_body<ST, CS_MODEL_REGULARISED, GAL, false, STAGED>(d, a, blockIdx.x);
+    bulk_body<ST, CS_MODEL_REGULARISED, GAL, false>(d, a, blockIdx.x);
 }
 
 // ---- 3. outlet resistances ----------------------------------------------------------------------------------------
@@ -844,11 +796,9 @@ __global__ void k_bc(const cs_step_desc d) { bc_body(d); }
 using StepFn = void (*)(const cs_step_desc, const int);
 
 template <int ST>
-StepFn pick_force(int model, int gal, bool force, int block, bool staged) {
-    if (model == CS_MODEL_REGULARISED && !force && block <= DENSE_BLOCK) {
-        if (staged) return gal ? k_bulk_dense<ST, true, true> : k_bulk_dense<ST, false, true>;
-        return gal ? k_bulk_dense<ST, true, false> : k_bulk_dense<ST, false, false>;
-    }
+StepFn pick_force(int model, int gal, bool force, int block) {
+    if (model == CS_MODEL_REGULARISED && !force && block <= DENSE_BLOCK)
+        return gal ? k_bulk_dense<ST, true> : k_bulk_dense<ST, false>;
     if (model == CS_MODEL_REGULARISED) {
         if (gal) return force ? k_bulk<ST, CS_MODEL_REGULARISED, true, true> : k_bulk<ST, CS_MODEL_REGULARISED, true, false>;
         return force ? k_bulk<ST, CS_MODEL_REGULARISED, false, true> : k_bulk<ST, CS_MODEL_REGULARISED, false, false>;
@@ -860,9 +810,7 @@ StepFn pick_force(int model, int gal, bool force, int block, bool staged) {
 template <int ST>
 StepFn pick_model(const cs_step_desc& d) {
     const bool force = d.force[0] != 0.0f || d.force[1] != 0.0f || d.force[2] != 0.0f;
-    // staged pulls: a 16-bit population's aligned 4-byte word must lie inside the buffer (even row length)
-    const bool staged = CS_STAGED_PULLS != 0 && (ST == CS_STORE_F32 || d.npad % 2 == 0);
-    return pick_force<ST>(d.model, d.gal, force, d.block ? d.block : MAX_BLOCK, staged);
+    return pick_force<ST>(d.model, d.gal, force, d.block ? d.block : MAX_BLOCK);
 }
 
 StepFn pick_bulk(const cs_step_desc& d) {
@@ -884,9 +832,8 @@ StepFn pick_boundary(const cs_step_desc& d) {
 int validate(const cs_step_desc* d) {
     if (!d) return fail(CS_ERR_ARG, "cs_step: null descriptor");
     if (d->n < 0 || d->n >= (int64_t(1) << 30)) return fail(CS_ERR_SIZE, "cs_step: n = %lld", (long long)d->n);
-    if (d->gmax < 0 || d->npad < d->n + d->gmax || int64_t(Q) * d->npad >= (int64_t(1) << 31))
-        return fail(CS_ERR_SIZE, "cs_step: npad %lld must be at least n + gmax with 27 * npad < 2^31",
-                    (long long)d->npad);
+    if (d->gmax < 0 || d->npad != d->n + d->gmax || int64_t(Q) * d->npad >= (int64_t(1) << 31))
+        return fail(CS_ERR_SIZE, "cs_step: npad %lld must be n + gmax with 27 * npad < 2^31", (long long)d->npad);
     if (d->gblock[0] != 0) return fail(CS_ERR_ARG, "cs_step: gblock[0] = %d", d->gblock[0]);
     for (int i = 0; i < Q; ++i) {
         const int64_t w = int64_t(d->gblock[i + 1]) - d->gblock[i];
@@ -1133,7 +1080,7 @@ __global__ void __launch_bounds__(MAX_BLOCK, MIN_BLOCKS) k_bulk_batch(const __gr
 // of at most 128 threads, compiled like k_bulk_dense for 9 blocks per SM, which the persistent loop's state does not
 // leave registers for. The block finds its instance by a binary search over the item prefix in the parameters.
 template <int ST, bool GAL>
-__global__ void __launch_bounds__(DENSE_BLOCK, BATCH_DENSE_MIN_BLOCKS) k_bulk_batch_dense(const __grid_constant__ BatchGroup g,
+__global__ void __launch_bounds__(DENSE_BLOCK, DENSE_MIN_BLOCKS) k_bulk_batch_dense(const __grid_constant__ BatchGroup g,
                                                                                   const int a) {
     const int item = int(blockIdx.x);
     const int inst = find_instance(g.bulk_prefix, g.n_inst, item);

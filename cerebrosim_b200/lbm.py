@@ -245,7 +245,7 @@ class Solver:
                 check(lib.cs_links_count(_ptr(nbr), N, _ptr(scratch), ghosts, sp))
                 self.ghosts = [int(x) for x in ghosts]
                 self.gmax = max(self.ghosts) if N else 0
-                self.npad = N + self.gmax + (N + self.gmax) % 2      # even rows: see cs_step_desc.npad
+                self.npad = N + self.gmax
                 gcols = max(1, self.gmax)
                 self.links = torch.empty((Q, N), dtype=torch.int32, device=dev)
                 self.gnode = torch.full((Q, gcols), -1, dtype=torch.int32, device=dev)

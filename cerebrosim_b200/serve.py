@@ -50,6 +50,7 @@ class Request:
         self.steps_total = 0
         self.steps_enq = 0
         self.evicted = None          # beat after which the request was evicted for diverging
+        self.beat_flags = []         # device flags of non-finite densities, one per enqueued beat end
 
     @property
     def queue_wait(self):
@@ -84,7 +85,8 @@ class Server:
     (a recalibrated drive: recalibrate_on_beat) applies from the next beat's first step.
 
     Divergence: at every beat end (before on_beat) a request's densities are checked for non-finite values
-    (simulate.py:321-322 raises there); a request that has diverged is evicted at once — its steps stop, its slot and
+    (simulate.py:321-322 raises there) by a reduction enqueued on the batch stream right after the beat's last
+    step; a request that has diverged is evicted at once — its steps stop, its slot and
     budget are released, and it ends with ok = False and `evicted` = the beat — while the others go on unchanged.
 
     log(record): called at every beat end with a JSON-ready dict — request id, beat, device time (s), the beat's
@@ -139,12 +141,15 @@ class Server:
                 r.fields = s.fields()
         r.solver = None
 
+    def _flag_beat(self, batch, r):
+        """Enqueue, on the batch stream right after the chunk that ends one of r's beats, a device flag of whether
+        any of r's densities is non-finite (read once that chunk has completed)."""
+        with torch.cuda.stream(batch.stream):
+            r.beat_flags.append(torch.isfinite(r.solver.rho).logical_not().any())
+
     def _finite(self, r):
-        """Densities all finite? Reduced on the side stream, which does not wait for the batch: chunks enqueued
-        after this beat may be running, and a value from any later step is as good (a non-finite density stays
-        non-finite)."""
-        with torch.cuda.stream(self._side):
-            return bool(torch.isfinite(r.solver.rho).all().item())
+        """Densities all finite at the beat end just completed (the oldest flag `_flag_beat` enqueued)."""
+        return not (r.beat_flags and bool(r.beat_flags.pop(0).item()))
 
     def _evict(self, r, beat, t):
         """Stop a diverged request: leave the batch once the chunks already enqueued for it have run, release its
@@ -239,12 +244,14 @@ class Server:
                 self._drain(inflight, base, start, active)
             if active and batch.members:
                 batch.run(self.chunk, chunk=self.graph_chunk)
-                ev = torch.cuda.Event(enable_timing=True)
-                ev.record(batch.stream)
                 snap = []
                 for r in active:
                     r.steps_enq += self.chunk
                     snap.append((r, r.steps_enq))
+                    if r.steps_enq % self.steps_per_beat == 0 and r.steps_enq < r.steps_total:
+                        self._flag_beat(batch, r)
+                ev = torch.cuda.Event(enable_timing=True)
+                ev.record(batch.stream)
                 inflight.append((ev, snap))
                 for r in [r for r in active if r.steps_enq >= r.steps_total]:
                     batch.remove(r.solver, sync=False)

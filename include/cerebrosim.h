@@ -163,8 +163,7 @@ int cs_compress_expand(const int32_t* lcode, const int32_t* segdelta, const int3
 
 typedef struct cs_step_desc {
     int64_t n;               /* fluid nodes */
-    int64_t npad;            /* population row length, at least n + gmax; 27 * npad < 2^31 (an even length lets the
-                              * 16-bit step stage its pulls through shared memory) */
+    int64_t npad;            /* population row length, n + gmax; 27 * npad < 2^31 */
     int64_t gmax;            /* ghost slots per direction */
     int32_t storage;         /* CS_STORE_* */
     int32_t model;           /* CS_MODEL_* (lbm.py:359) */
