@@ -498,34 +498,36 @@ def main():
     del warm
     torch.cuda.synchronize()
     barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t_host = [time.perf_counter()]
-    e0.record()
-    s2 = lbm.Solver(host, nu_lu(), model="regularised", device=dev, storage=args.storage, **shape)
-    configure(s2)
-    t_host.append(time.perf_counter())
-    s2.run(args.steps)
-    s2.synchronize()
-    t_host.append(time.perf_counter())
-    p_h, u_h = s2.fields()
-    e1.record()
-    torch.cuda.synchronize()
-    t_host.append(time.perf_counter())
-    e2e_secs = max_over_ranks(e0.elapsed_time(e1) * 1e-3)
-    d2h = p_h.nbytes + u_h.nbytes
+    def e2e_once():
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t_host = [time.perf_counter()]
+        e0.record()
+        s2 = lbm.Solver(host, nu_lu(), model="regularised", device=dev, storage=args.storage, **shape)
+        configure(s2)
+        t_host.append(time.perf_counter())
+        s2.run(args.steps)
+        s2.synchronize()
+        t_host.append(time.perf_counter())
+        p_h, u_h = s2.fields()
+        e1.record()
+        torch.cuda.synchronize()
+        t_host.append(time.perf_counter())
+        parts = {"construct": (t_host[1] - t_host[0]) * 1e3, "run": (t_host[2] - t_host[1]) * 1e3,
+                 "fields": (t_host[3] - t_host[2]) * 1e3}
+        return e0.elapsed_time(e1) * 1e-3, parts, p_h.nbytes + u_h.nbytes
+
+    # three end-to-end runs (each: construction from the host tables, the K steps, the read-back); the median is
+    # reported, so that one run disturbed by the host (a construction of 23 ms instead of 4 was seen) does not
+    # stand for the path
+    runs = [e2e_once() for _ in range(3)]
+    order_ = sorted(range(3), key=lambda k: runs[k][0])
+    secs_med, parts, d2h = runs[order_[1]]
+    e2e_secs = max_over_ranks(secs_med)
     e2e = {"value": world * N * args.steps / e2e_secs / 1e6, "unit": "MLUPS",
            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
            "definition": "Solver(lat) from pinned host tables + run(K) in CUDA graphs + fields() readback, "
-                         "no L2 flush",
-           "parts_ms": {"construct": (t_host[1] - t_host[0]) * 1e3, "run": (t_host[2] - t_host[1]) * 1e3,
-                        "fields": (t_host[3] - t_host[2]) * 1e3}}
-
-    # the batched sweep and the served stream: every rank runs its share (the same collective calls on every rank)
-    extra = {}
-    if args.sweep_steps > 0:
-        extra["batched"] = bench_sweep(args, dev, peak, rep)
-    if args.serve_requests > 0:
-        extra["served"] = bench_served(args, dev, rep)
+                         "no L2 flush; median of three runs",
+           "parts_ms": parts, "runs_ms": [r[0] * 1e3 for r in runs]}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
