@@ -402,7 +402,8 @@ class Solver:
         full, rest = divmod(int(steps), chunk)
         cur_stream = torch.cuda.current_stream(self.dev)
         self.stream.wait_stream(cur_stream)
-        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+        with torch.cuda.nvtx.range(f"Solver.run {steps} steps, {self.N} nodes"), torch.cuda.device(self.dev), \
+                torch.cuda.stream(self.stream):
             if full:
                 key = (self.cur, chunk)
                 if key not in self.graphs:

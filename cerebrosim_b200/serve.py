@@ -174,6 +174,7 @@ class Server:
                 continue
             if steps % self.steps_per_beat == 0:
                 r.beat_end.append(t)
+                torch.cuda.nvtx.mark(f"request {r.id} beat {steps // self.steps_per_beat} done")
                 if self.log is not None:
                     lat = r.beat_latencies()[-1]
                     self.log({"request": r.id, "beat": steps // self.steps_per_beat, "t_s": t, "latency_s": lat,
@@ -243,7 +244,9 @@ class Server:
                 # final state and what it changes applies from the next beat's first step (simulate.py:330-337)
                 self._drain(inflight, base, start, active)
             if active and batch.members:
-                batch.run(self.chunk, chunk=self.graph_chunk)
+                # an NVTX range per scheduling round (members, steps) for a timeline profiler
+                with torch.cuda.nvtx.range(f"serve chunk: {len(active)} requests x {self.chunk} steps"):
+                    batch.run(self.chunk, chunk=self.graph_chunk)
                 snap = []
                 for r in active:
                     r.steps_enq += self.chunk
