@@ -529,6 +529,13 @@ def main():
                          "no L2 flush; median of three runs",
            "parts_ms": parts, "runs_ms": [r[0] * 1e3 for r in runs]}
 
+    # the batched sweep and the served stream: every rank runs its share (the same collective calls on every rank)
+    extra = {}
+    if args.sweep_steps > 0:
+        extra["batched"] = bench_sweep(args, dev, peak, rep)
+    if args.serve_requests > 0:
+        extra["served"] = bench_served(args, dev, rep)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": mean_step * 1e3, "higher_is_better": True,
