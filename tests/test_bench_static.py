@@ -14,6 +14,7 @@ def test_bench_reads_no_undefined_name():
     module |= {t.id for n in tree.body if isinstance(n, ast.Assign) for t in n.targets if isinstance(t, ast.Name)}
     module |= {(a.asname or a.name).split(".")[0] for n in tree.body if isinstance(n, (ast.Import, ast.ImportFrom))
                for a in n.names}
+    module |= {"__file__", "__name__"}
     for fn in (n for n in tree.body if isinstance(n, ast.FunctionDef)):
         defined, used = set(), set()
         for node in ast.walk(fn):
@@ -23,6 +24,8 @@ def test_bench_reads_no_undefined_name():
                 defined.add(node.name)
             elif isinstance(node, ast.arg):
                 defined.add(node.arg)
+            elif isinstance(node, ast.ExceptHandler) and node.name:
+                defined.add(node.name)
             elif isinstance(node, (ast.Import, ast.ImportFrom)):
                 defined |= {(a.asname or a.name).split(".")[0] for a in node.names}
         missing = sorted(u for u in used - defined - module if not hasattr(builtins, u))
