@@ -92,6 +92,7 @@ class Clocks:
 
     def __init__(self, index):
         self.p = None
+        self.index = index
         self.path = f"/tmp/cs_clocks_{os.getpid()}.csv"
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={self.Q}",
@@ -107,7 +108,16 @@ class Clocks:
         self.p.terminate()
         self.p.wait()
         rows = []
-        for line in open(self.path):
+        lines = list(open(self.path))
+        if not lines:
+            # a timed region shorter than the sampler's start-up: one query right after it
+            try:
+                lines = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                        "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                       timeout=30).stdout.splitlines()
+            except (OSError, subprocess.SubprocessError):
+                lines = []
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) == 7:
                 try:
@@ -443,6 +453,9 @@ def main():
         s.cur = 1 - s.cur
         s.steps += 1
 
+    # the clock sampler starts before the warm-up (nvidia-smi takes longer to start than a short timed region
+    # lasts); its samples cover the warm-up and the timed steps of the same workload
+    clocks = Clocks(local)
     with torch.cuda.stream(stream):
         for k in range(args.warmup):
             flush(k)
@@ -453,7 +466,6 @@ def main():
         whole0, whole1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
         torch.cuda.synchronize()
-        clocks = Clocks(local)
         whole0.record(stream)
         for k in range(args.steps):
             flush(k)
