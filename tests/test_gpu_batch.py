@@ -185,3 +185,18 @@ def test_coupled_runs_are_reproducible(golden):
     same(r1, r2)
     assert np.abs(r1.Qlast.numpy()).max() > 0
     assert torch.equal(r1.f[r1.cur], r2.f[r2.cur])
+
+
+@pytest.mark.parametrize("schedule", ["fused", "by-instance", "concurrent:2"])
+def test_graph_per_heartbeat_prepared_ahead(golden, schedule):
+    """A heartbeat's steps as one CUDA graph per member (or per 400 steps for the fused schedule), captured by
+    prepare() before the run: the same fields, bit for bit, as the same steps in graphs of 40."""
+    beat = 600
+    ref = [make(golden, n, c, k) for n, c, k in SPECS]
+    got = [make(golden, n, c, k) for n, c, k in SPECS]
+    BatchSolver(ref, schedule=schedule).run(2 * beat, chunk=40)
+    b = BatchSolver(got, schedule=schedule)
+    b.prepare(beat)
+    b.run(2 * beat, chunk=beat)
+    for a, m in zip(ref, got):
+        same(a, m)
