@@ -198,7 +198,10 @@ class Solver:
         self.dev = _device(device)
         self.lat = lat
         self.N = N = int(lat["nbr"].shape[1])
-        perm = node_order(lat, order)
+        # the C-based split orders are found on the device once the tables are there (a host pass over the 27 x N
+        # table would cost more than the rest of the construction)
+        on_device = order in ("split", "boundary-first")
+        perm = None if on_device else node_order(lat, order)
         self.order = order
         self.tau = 3.0 * nu_lu + 0.5
         self.magic = float(magic)
@@ -214,74 +217,88 @@ class Solver:
             raise ValueError(f"block {self.block}: a multiple of 32 in 32..256")
         pop_dtype = {"f32": torch.float32, "f16": torch.float16, "bf16": torch.bfloat16}[storage]
         with torch.cuda.device(self.dev):
+            # set-up (uploads, table kernels, allocations) runs on the caller's stream, so that the caching
+            # allocator serves a Solver built after another one freed its tensors from the same pool; the steps
+            # run on a private stream, ordered after the set-up, and every tensor the steps use is recorded on it
             self.stream = torch.cuda.Stream(self.dev)
-            self.stream.wait_stream(torch.cuda.current_stream(self.dev))
-            sp = ctypes_void(self.stream.cuda_stream)
-            with torch.cuda.stream(self.stream):
-                dev = self.dev
-                tabs = lat.get("_dev") if isinstance(lat.get("_dev"), dict) else None
-                if tabs is not None and tabs["nbr"].device == dev:
-                    nbr, q, uin = tabs["nbr"], tabs["q"], tabs["uin"]
-                else:
-                    nbr = _upload(lat["nbr"], torch.int32, dev)
-                    q = _upload(lat["q"], torch.float32, dev)
-                    uin = _upload(lat["uin"], torch.float32, dev)
-                self.perm = self.inv = None
-                if perm is not None:
-                    # internal node k is the lattice's node perm[k]; sources renumbered through inv
-                    self.perm = torch.as_tensor(perm.astype(np.int64)).to(dev)
-                    self.inv = torch.empty_like(self.perm)
-                    self.inv[self.perm] = torch.arange(N, device=dev)
-                    src = nbr[:, self.perm]
-                    nbr = torch.where(src >= 0, self.inv[src.clamp(min=0)].to(torch.int32), src).contiguous()
-                    q = q[:, self.perm].contiguous()
-                    uin = uin[self.perm]
-                self.uin = uin.contiguous()
-                self.inl = (nbr == INLET).any(0).to(torch.int32) if N else torch.zeros(0, dtype=torch.int32, device=dev)
-                n_out = max(1, int(lat["n_outlets"]))
-                # step link tables: fluid pull sources, and a ghost slot per boundary link (csrc/links.cu)
-                scratch = torch.empty(max(1, int(lib.cs_links_scratch_bytes(N))), dtype=torch.uint8, device=dev)
-                ghosts = (ctypes.c_int64 * Q)()
-                check(lib.cs_links_count(_ptr(nbr), N, _ptr(scratch), ghosts, sp))
-                self.ghosts = [int(x) for x in ghosts]
-                self.gmax = max(self.ghosts) if N else 0
-                self.npad = N + self.gmax
-                gcols = max(1, self.gmax)
-                self.links = torch.empty((Q, N), dtype=torch.int32, device=dev)
-                self.gnode = torch.full((Q, gcols), -1, dtype=torch.int32, device=dev)
-                self.ginfo = torch.full((Q, gcols), WALL, dtype=torch.int32, device=dev)
-                self.gq = torch.full((Q, gcols), -1.0, dtype=torch.float32, device=dev)
-                status = torch.empty(2, dtype=torch.int64, device=dev)
-                check(lib.cs_links_fill(_ptr(nbr), _ptr(q), N, n_out, self.gmax, _ptr(scratch), _ptr(self.links),
-                                        _ptr(self.gnode), _ptr(self.ginfo), _ptr(self.gq), _ptr(status), sp))
-                del scratch
-                # compressed connectivity (csrc/compress.cu): 4 bytes per regular node instead of 108
-                scratch = torch.empty(max(1, int(lib.cs_compress_scratch_bytes(N))), dtype=torch.uint8, device=dev)
-                n_seg, n_irr = ctypes.c_int64(0), ctypes.c_int64(0)
-                check(lib.cs_compress_count(_ptr(self.links), N, _ptr(scratch), ctypes.byref(n_seg),
-                                            ctypes.byref(n_irr), sp))
-                self.n_seg, self.n_irr = int(n_seg.value), int(n_irr.value)
-                self.lcode = torch.empty(max(1, N), dtype=torch.int32, device=dev)
-                self.segdelta = torch.empty((max(1, self.n_seg), SEG_STRIDE), dtype=torch.int32, device=dev)
-                self.irr = torch.empty((Q, max(1, self.n_irr)), dtype=torch.int32, device=dev)
-                assert self.segdelta.numel() >= self.n_seg * SEG_STRIDE and self.irr.numel() >= self.n_irr * Q
-                assert self.segdelta.data_ptr() % 16 == 0   # rows are read with 128-bit loads
-                check(lib.cs_compress_fill(_ptr(self.links), N, self.n_seg, self.n_irr, _ptr(scratch),
-                                           _ptr(self.lcode), _ptr(self.segdelta), _ptr(self.irr), sp))
-                self.stream.synchronize()
-                del scratch
-                self.links = None                          # the full 27 x N table is not needed by the step
-                self.f = [torch.zeros((Q, self.npad), dtype=pop_dtype, device=dev) for _ in range(2)]
-                self.vel = [torch.zeros((3, N), dtype=torch.float32, device=dev) for _ in range(2)]
-                self.vels = [v.T for v in self.vel]
-                self.rho = torch.zeros(N, dtype=torch.float32, device=dev)
-                self.p_out = torch.zeros(n_out, dtype=torch.float32, device=dev)
-                self.p_out64 = torch.zeros(n_out, dtype=torch.float64, device=dev)
-                # 1 / tau per node, negated on cells with an inlet link (the kernel's inlet-cell flag)
-                self._om_sign = 1.0 - 2.0 * self.inl.to(torch.float32)
-                self.om = torch.full((N,), 1.0 / self.tau, dtype=torch.float32, device=dev) * self._om_sign
-                self.tick = torch.zeros(2, dtype=torch.int32, device=dev)
-                self.drv = torch.zeros(1, dtype=torch.float32, device=dev)
+            setup = torch.cuda.current_stream(self.dev)
+            sp = ctypes_void(setup.cuda_stream)
+            dev = self.dev
+            tabs = lat.get("_dev") if isinstance(lat.get("_dev"), dict) else None
+            if tabs is not None and tabs["nbr"].device == dev:
+                nbr, q, uin = tabs["nbr"], tabs["q"], tabs["uin"]
+            else:
+                nbr = _upload(lat["nbr"], torch.int32, dev)
+                q = _upload(lat["q"], torch.float32, dev)
+                uin = _upload(lat["uin"], torch.float32, dev)
+            self.perm = self.inv = None
+            if on_device and N:
+                bnd = (nbr < 0).any(0)
+                parts = [torch.nonzero(~bnd).flatten(), torch.nonzero(bnd).flatten()]
+                perm_d = torch.cat(parts[::-1] if order == "boundary-first" else parts)
+                if not bool((perm_d == torch.arange(N, device=dev)).all()):
+                    perm = perm_d
+            if perm is not None:
+                # internal node k is the lattice's node perm[k]; sources renumbered through inv
+                self.perm = perm if isinstance(perm, torch.Tensor) else torch.as_tensor(perm.astype(np.int64)).to(dev)
+                self.inv = torch.empty_like(self.perm)
+                self.inv[self.perm] = torch.arange(N, device=dev)
+                src = nbr[:, self.perm]
+                nbr = torch.where(src >= 0, self.inv[src.clamp(min=0)].to(torch.int32), src).contiguous()
+                q = q[:, self.perm].contiguous()
+                uin = uin[self.perm]
+            self.uin = uin.contiguous()
+            self.inl = (nbr == INLET).any(0).to(torch.int32) if N else torch.zeros(0, dtype=torch.int32, device=dev)
+            n_out = max(1, int(lat["n_outlets"]))
+            # step link tables: fluid pull sources, and a ghost slot per boundary link (csrc/links.cu)
+            scratch = torch.empty(max(1, int(lib.cs_links_scratch_bytes(N))), dtype=torch.uint8, device=dev)
+            ghosts = (ctypes.c_int64 * Q)()
+            check(lib.cs_links_count(_ptr(nbr), N, _ptr(scratch), ghosts, sp))
+            self.ghosts = [int(x) for x in ghosts]
+            self.gmax = max(self.ghosts) if N else 0
+            self.npad = N + self.gmax
+            gcols = max(1, self.gmax)
+            self.links = torch.empty((Q, N), dtype=torch.int32, device=dev)
+            self.gnode = torch.full((Q, gcols), -1, dtype=torch.int32, device=dev)
+            self.ginfo = torch.full((Q, gcols), WALL, dtype=torch.int32, device=dev)
+            self.gq = torch.full((Q, gcols), -1.0, dtype=torch.float32, device=dev)
+            status = torch.empty(2, dtype=torch.int64, device=dev)
+            check(lib.cs_links_fill(_ptr(nbr), _ptr(q), N, n_out, self.gmax, _ptr(scratch), _ptr(self.links),
+                                    _ptr(self.gnode), _ptr(self.ginfo), _ptr(self.gq), _ptr(status), sp))
+            del scratch
+            # compressed connectivity (csrc/compress.cu): 4 bytes per regular node instead of 108
+            scratch = torch.empty(max(1, int(lib.cs_compress_scratch_bytes(N))), dtype=torch.uint8, device=dev)
+            n_seg, n_irr = ctypes.c_int64(0), ctypes.c_int64(0)
+            check(lib.cs_compress_count(_ptr(self.links), N, _ptr(scratch), ctypes.byref(n_seg),
+                                        ctypes.byref(n_irr), sp))
+            self.n_seg, self.n_irr = int(n_seg.value), int(n_irr.value)
+            self.lcode = torch.empty(max(1, N), dtype=torch.int32, device=dev)
+            self.segdelta = torch.empty((max(1, self.n_seg), SEG_STRIDE), dtype=torch.int32, device=dev)
+            self.irr = torch.empty((Q, max(1, self.n_irr)), dtype=torch.int32, device=dev)
+            assert self.segdelta.numel() >= self.n_seg * SEG_STRIDE and self.irr.numel() >= self.n_irr * Q
+            assert self.segdelta.data_ptr() % 16 == 0   # rows are read with 128-bit loads
+            check(lib.cs_compress_fill(_ptr(self.links), N, self.n_seg, self.n_irr, _ptr(scratch),
+                                       _ptr(self.lcode), _ptr(self.segdelta), _ptr(self.irr), sp))
+            setup.synchronize()
+            del scratch
+            self.links = None                          # the full 27 x N table is not needed by the step
+            self.f = [torch.zeros((Q, self.npad), dtype=pop_dtype, device=dev) for _ in range(2)]
+            self.vel = [torch.zeros((3, N), dtype=torch.float32, device=dev) for _ in range(2)]
+            self.vels = [v.T for v in self.vel]
+            self.rho = torch.zeros(N, dtype=torch.float32, device=dev)
+            self.p_out = torch.zeros(n_out, dtype=torch.float32, device=dev)
+            self.p_out64 = torch.zeros(n_out, dtype=torch.float64, device=dev)
+            # 1 / tau per node, negated on cells with an inlet link (the kernel's inlet-cell flag)
+            self._om_sign = 1.0 - 2.0 * self.inl.to(torch.float32)
+            self.om = torch.full((N,), 1.0 / self.tau, dtype=torch.float32, device=dev) * self._om_sign
+            self.tick = torch.zeros(2, dtype=torch.int32, device=dev)
+            self.drv = torch.zeros(1, dtype=torch.float32, device=dev)
+            for t in (self.perm, self.inv, self.uin, self.inl, self.gnode, self.ginfo, self.gq, self.lcode,
+                      self.segdelta, self.irr, *self.f, *self.vel, self.rho, self.p_out, self.p_out64,
+                      self._om_sign, self.om, self.tick, self.drv):
+                if t is not None:
+                    t.record_stream(self.stream)
+            self.stream.wait_stream(setup)
         self.force = (0.0, 0.0, 0.0)
         self.graphs = {}
         self.set_drive([1.0])
@@ -444,7 +461,8 @@ class Solver:
         """(pressure, velocity) per cell of the lattice (its node order, whatever the internal one), lattice units,
         as NumPy (lbm.py:450-452)."""
         self.stream.synchronize()
-        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
+        # on the caller's stream (the steps are done): its pool holds the construction's freed blocks
+        with torch.cuda.device(self.dev):
             rho, vel = self.rho, self.vel[self.cur]
             if self.inv is not None:
                 rho, vel = rho[self.inv], vel[:, self.inv]
@@ -513,7 +531,10 @@ class Solver:
             pass
 
 
-ORDERS = ("c", "axis", "morton", "split", "axis-split")
+ORDERS = ("c", "axis", "morton", "split", "axis-split", "boundary-first", "axis-boundary-first")
+# orders that separate the nodes with a boundary link from the others, and on which base order
+_SPLITS = {"split": ("c", False), "axis-split": ("axis", False), "boundary-first": ("c", True),
+           "axis-boundary-first": ("axis", True)}
 
 
 def node_order(lat, order="c"):
@@ -521,17 +542,20 @@ def node_order(lat, order="c"):
     C order. "axis": C order with the axis of largest extent varying fastest (long runs along a vessel); "morton":
     Z-order curve of the grid coordinates; "split" / "axis-split": C / axis order with the nodes that have a
     boundary link moved after all others (so the boundary-link kernel reads consecutive nodes and the bulk
-    kernel's warps are all plain or all boundary)."""
+    kernel's warps are all plain or all boundary); "boundary-first" / "axis-boundary-first": the same with those
+    nodes first, so that the bulk grid's slowest blocks (irregular connectivity, inlet cells) start first and the
+    plain blocks fill its last wave."""
     if order not in ORDERS:
         raise ValueError(f"order {order!r}: one of {ORDERS}")
     if order == "c" or lat["nbr"].shape[1] == 0:
         return None
     c = np.asarray(lat["coords"], np.int64)
-    if order.endswith("split"):
-        base = node_order(lat, "axis") if order == "axis-split" else None
+    if order in _SPLITS:
+        base_order, first = _SPLITS[order]
+        base = node_order(lat, base_order) if base_order != "c" else None
         base = np.arange(len(c)) if base is None else base
         bnd = (np.asarray(lat["nbr"]) < 0).any(0)[base]
-        perm = np.concatenate([base[~bnd], base[bnd]])
+        perm = np.concatenate([base[bnd], base[~bnd]] if first else [base[~bnd], base[bnd]])
         return None if np.array_equal(perm, np.arange(len(perm))) else perm
     if order == "axis":
         ext = c.max(0) - c.min(0)

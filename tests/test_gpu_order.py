@@ -28,7 +28,7 @@ def test_orders_give_identical_fields(golden, storage):
     configure(ref)
     ref.run(301)
     p0, u0 = ref.fields()
-    for order in ("axis", "morton", "split", "axis-split"):
+    for order in ("axis", "morton", "split", "axis-split", "boundary-first", "axis-boundary-first"):
         s = lbm.Solver(lat, 0.02, model="regularised", storage=storage, order=order)
         assert order == "axis" or s.perm is not None
         configure(s)

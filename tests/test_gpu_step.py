@@ -104,7 +104,7 @@ def test_headline_pipe_16bit_at_full_size(storage, bound):
 def test_stenosed_artery_at_full_size():
     """The batched / served workloads' vessel at its full size: the generated stenosed artery of seed 3 at 0.05 mm
     (1,567,027 nodes; Bouzidi walls, Fourier velocity inlet, two pressure outlets, sponge), 1000 FP32 steps against
-    the oracle on the same tables, in the lattice's C order and in the vessel-axis order the autotuner picks."""
+    the oracle on the same tables, in the lattice's C order and in the vessel-axis orders the autotuner picks."""
     from cerebrosim_b200 import workloads
     spec = {"seed": 3, "stenosis": 0.7, "pressure": 95.0}
     lat = workloads.lattice(workloads.stenosed_vessel(3), 0.05)
@@ -112,7 +112,7 @@ def test_stenosed_artery_at_full_size():
     r = OracleSolver(lat, (0.52 - 0.5) / 3.0, model="regularised")
     workloads.configure(r, spec, lat, period=8000)
     r.run(STEPS)
-    for order in ("c", "axis-split"):
+    for order in ("c", "axis-split", "axis-boundary-first"):
         g = workloads.make_solver(spec, lat, period=8000, order=order)
         g.run(STEPS)
         compare(g, r)

@@ -108,3 +108,19 @@ def test_split_order_puts_boundary_nodes_last():
     k = int((~bnd).sum())
     assert not bnd[perm[:k]].any() and bnd[perm[k:]].all()
     assert np.all(np.diff(perm[:k]) > 0) and np.all(np.diff(perm[k:]) > 0)      # C order within each part
+
+
+def test_boundary_first_order_puts_boundary_nodes_first():
+    from cerebrosim_b200 import cases, lbm
+    from oracle import lattice_ref as L
+    lat = L.build_lattice(**cases.lattice_args(cases.case("open_pipe_straight_D20")))
+    bnd = (lat["nbr"] < 0).any(0)
+    k = int(bnd.sum())
+    perm = lbm.node_order(lat, "boundary-first")
+    assert np.array_equal(np.sort(perm), np.arange(len(perm)))
+    assert bnd[perm[:k]].all() and not bnd[perm[k:]].any()
+    assert np.all(np.diff(perm[:k]) > 0) and np.all(np.diff(perm[k:]) > 0)      # C order within each part
+    axis = lbm.node_order(lat, "axis")
+    axis = np.arange(len(bnd)) if axis is None else axis              # None: the axis order is the C order
+    perm = lbm.node_order(lat, "axis-boundary-first")
+    assert np.array_equal(perm, np.concatenate([axis[bnd[axis]], axis[~bnd[axis]]]))
