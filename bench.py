@@ -180,15 +180,20 @@ def run_reference(args):
 
 def artery_line(storage, steps, warmup, dev, peak, flush):
     """The single-vessel configuration at full size: the generated stenosed artery of seed 3 at 0.05 mm (1,567,027
-    nodes), one solver, `steps` steps timed one by one with the L2 flushed before each (as the headline), and the
-    same steps back to back."""
+    nodes), one solver in the node order the autotuner picks for it, `steps` steps timed one by one with the L2
+    flushed before each (as the headline), and the same steps back to back."""
     import ctypes
 
     import torch
 
-    from cerebrosim_b200 import _lib
+    from cerebrosim_b200 import _lib, autotune, workloads
     lib = _lib.load()
-    s = case_solver("artery:3", storage, device=dev)
+    spec = {"seed": 3, "stenosis": 0.7, "pressure": 95.0}
+    lat = workloads.lattice(workloads.stenosed_vessel(3), 0.05, device=dev)
+    best, _ = autotune.tune(lat, (0.52 - 0.5) / 3.0, configure=lambda x: workloads.configure(x, spec, lat),
+                            storage=storage, blocks=(128,), orders=("c", "axis-split", "axis-boundary-first"),
+                            steps=100, warmup=30, device=dev, model="regularised")
+    s = workloads.make_solver(spec, lat, storage=storage, device=dev, order=best["order"])
     descs = [s._desc(), s._desc()]
     sp = ctypes.c_void_p(s.stream.cuda_stream)
 
@@ -221,7 +226,8 @@ def artery_line(storage, steps, warmup, dev, peak, flush):
     bplu = BPLU[storage]
     out = {"workload": "generated stenosed artery, seed 3, 0.05 mm (70 % cosine stenosis, 40 degree side branch, "
                        "Fourier velocity inlet, two pressure outlets, sponge; tau 0.52)",
-           "nodes": s.N, "storage": storage, "block": s.block, "steps": steps, "value": mlups, "unit": "MLUPS",
+           "nodes": s.N, "storage": storage, "block": s.block, "order": s.order, "steps": steps, "value": mlups,
+           "unit": "MLUPS",
            "ms_per_step": secs / steps * 1e3, "hbm_gbs": bplu * mlups / 1e3, "frac": bplu * mlups / 1e3 / peak,
            "bytes_per_update": bplu, "l2": "flushed between timed steps, as the headline",
            "back_to_back": {"ms_per_step": b2b / steps * 1e3, "value": s.N * steps / b2b / 1e6, "unit": "MLUPS"},
@@ -230,22 +236,23 @@ def artery_line(storage, steps, warmup, dev, peak, flush):
     return out
 
 
-def case_solver(name, storage, block=None, device=None):
+def case_solver(name, storage, block=None, device=None, order="c"):
     """Solver of a named case: the pulsatile-pipe set-up for open pipes (plug inlet, its drive, pressure outlet,
     tau 0.55), a body force for periodic pipes, or artery:SEED — the generated stenosed artery of that seed at
-    0.05 mm (70 % stenosis, side branch, Fourier inflow, tau 0.52)."""
+    0.05 mm (70 % stenosis, side branch, Fourier inflow, tau 0.52); `order`: the internal node order."""
     from cerebrosim_b200 import cases, lbm, workloads
     if name.startswith("artery:"):
         seed = int(name.split(":")[1])
         spec = {"seed": seed, "stenosis": 0.7, "pressure": 95.0}
         lat = workloads.lattice(workloads.stenosed_vessel(seed), 0.05, device=device)
-        return workloads.make_solver(spec, lat, storage=storage, block=block, device=device)
+        return workloads.make_solver(spec, lat, storage=storage, block=block, device=device, order=order)
     lat = lbm.build_lattice(**cases.lattice_args(cases.case(name)), device=device)
     if lat["n_outlets"] or any(o["kind"] == "inlet" for o in lat["openings"]):
-        s = lbm.Solver(cases.plug_inlet(lat), nu_lu(), model="regularised", storage=storage, block=block, device=device)
+        s = lbm.Solver(cases.plug_inlet(lat), nu_lu(), model="regularised", storage=storage, block=block,
+                       device=device, order=order)
         configure(s)
     else:
-        s = lbm.Solver(lat, nu_lu(), model="regularised", storage=storage, block=block, device=device)
+        s = lbm.Solver(lat, nu_lu(), model="regularised", storage=storage, block=block, device=device, order=order)
         s.set_force([0.0, 0.0, 1e-6])
     return s
 
@@ -253,14 +260,15 @@ def case_solver(name, storage, block=None, device=None):
 def run_profile(args):
     """--profile CASE: warm-up and timed steps of one case (CUDA graphs of 100 steps), one JSON line."""
     import torch
-    s = case_solver(args.profile, args.storage)
+    s = case_solver(args.profile, args.storage, order=args.order)
     s.run(args.warmup, chunk=100)
     s.synchronize()
     t = time.perf_counter()
     s.run(args.steps, chunk=100)
     s.synchronize()
     secs = time.perf_counter() - t
-    print(json.dumps({"case": args.profile, "nodes": s.N, "steps": args.steps, "storage": args.storage,
+    print(json.dumps({"case": args.profile, "order": args.order, "nodes": s.N, "steps": args.steps,
+                      "storage": args.storage,
                       "block": s.block, "mlups": s.N * args.steps / secs / 1e6, "ok": s.ok(),
                       "gpu": torch.cuda.get_device_name()}), flush=True)
 
@@ -397,6 +405,7 @@ def main():
                     help="run only CASE (a named lattice of cerebrosim_b200.cases, or artery:SEED for the generated "
                          "stenosed artery at 0.05 mm) for --warmup + --steps steps and print its throughput: the "
                          "command the ncu summaries are captured from")
+    ap.add_argument("--order", default="c", help="internal node order of --profile (lbm.ORDERS)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -425,12 +434,13 @@ def main():
     c = cases.case(WORKLOAD)
     lat = cases.plug_inlet(lbm.build_lattice(**cases.lattice_args(c), device=dev))
     N = lat["nbr"].shape[1]
-    # block size chosen by the autotuner (short timed runs of each candidate on this lattice); the reference's node
-    # order (the split order gains ~3 % back to back but nothing with a cold L2, and costs the end-to-end path its
-    # renumbering)
+    # block size and node order chosen by the autotuner (short timed runs of each candidate on this lattice): the
+    # reference's C order, or C order with the nodes that have a boundary link first (found on the device, so the
+    # end-to-end path pays no host pass for it)
     from cerebrosim_b200 import autotune
     tuned, tune_table = autotune.tune(lat, nu_lu(), configure=configure, storage=args.storage, blocks=(64, 128, 256),
-                                      orders=("c",), steps=400, warmup=100, device=dev, model="regularised")
+                                      orders=("c", "boundary-first"), steps=400, warmup=100, device=dev,
+                                      model="regularised")
     shape = {"block": tuned["block"], "order": tuned["order"]}
     s = lbm.Solver(lat, nu_lu(), model="regularised", device=dev, storage=args.storage, **shape)
     configure(s)
