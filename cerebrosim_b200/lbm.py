@@ -225,8 +225,20 @@ class Solver:
             sp = ctypes_void(setup.cuda_stream)
             dev = self.dev
             tabs = lat.get("_dev") if isinstance(lat.get("_dev"), dict) else None
+            side = None
             if tabs is not None and tabs["nbr"].device == dev:
                 nbr, q, uin = tabs["nbr"], tabs["q"], tabs["uin"]
+            elif all(isinstance(lat[k], torch.Tensor) for k in ("nbr", "q", "uin")):
+                # host tensors (pinned: asynchronous copies): q and uin cross PCIe on a side stream while the work
+                # that needs only nbr (renumbering, the ghost count) runs; the set-up waits for them before use
+                nbr = _upload(lat["nbr"], torch.int32, dev)
+                q = torch.empty(tuple(lat["q"].shape), dtype=torch.float32, device=dev)
+                uin = torch.empty(tuple(lat["uin"].shape), dtype=torch.float32, device=dev)
+                side = torch.cuda.Stream(dev)
+                side.wait_stream(setup)
+                with torch.cuda.stream(side):
+                    q.copy_(lat["q"], non_blocking=True)
+                    uin.copy_(lat["uin"], non_blocking=True)
             else:
                 nbr = _upload(lat["nbr"], torch.int32, dev)
                 q = _upload(lat["q"], torch.float32, dev)
@@ -245,15 +257,18 @@ class Solver:
                 self.inv[self.perm] = torch.arange(N, device=dev)
                 src = nbr[:, self.perm]
                 nbr = torch.where(src >= 0, self.inv[src.clamp(min=0)].to(torch.int32), src).contiguous()
-                q = q[:, self.perm].contiguous()
-                uin = uin[self.perm]
-            self.uin = uin.contiguous()
             self.inl = (nbr == INLET).any(0).to(torch.int32) if N else torch.zeros(0, dtype=torch.int32, device=dev)
             n_out = max(1, int(lat["n_outlets"]))
             # step link tables: fluid pull sources, and a ghost slot per boundary link (csrc/links.cu)
             scratch = torch.empty(max(1, int(lib.cs_links_scratch_bytes(N))), dtype=torch.uint8, device=dev)
             ghosts = (ctypes.c_int64 * Q)()
             check(lib.cs_links_count(_ptr(nbr), N, _ptr(scratch), ghosts, sp))
+            if side is not None:
+                setup.wait_stream(side)
+            if self.perm is not None:
+                q = q[:, self.perm].contiguous()
+                uin = uin[self.perm]
+            self.uin = uin.contiguous()
             self.ghosts = [int(x) for x in ghosts]
             self.gmax = max(self.ghosts) if N else 0
             self.npad = N + self.gmax

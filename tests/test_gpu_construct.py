@@ -74,3 +74,21 @@ def test_constructions_reuse_device_memory(pipe):
     grown = torch.cuda.memory_reserved() - r0
     assert footprint > 64 << 20
     assert grown < footprint // 4, f"reserve grew by {grown >> 20} MiB over three constructions"
+
+
+@pytest.mark.parametrize("order", ["c", "boundary-first"])
+def test_pinned_host_tables(pipe, order):
+    """From pinned host tensors (the end-to-end path: two of the three tables are copied on a side stream while the
+    set-up works on the first) the solver's tables and fields are those built from the device tables."""
+    host = {k: v for k, v in pipe.items() if k != "_dev"}
+    for k in ("nbr", "q", "uin"):
+        host[k] = torch.from_numpy(np.ascontiguousarray(pipe[k])).pin_memory()
+    a = solver(pipe, order=order)
+    b = solver(host, order=order)
+    for name in ("lcode", "segdelta", "irr", "gnode", "ginfo", "gq", "uin", "om"):
+        assert torch.equal(getattr(a, name), getattr(b, name)), name
+    for s in (a, b):
+        s.run(100)
+    pa, ua = a.fields()
+    pb, ub = b.fields()
+    assert np.array_equal(pa, pb) and np.array_equal(ua, ub)
