@@ -200,9 +200,9 @@ class Solver:
         self.dev = _device(device)
         self.lat = lat
         self.N = N = int(lat["nbr"].shape[1])
-        # the C-based split orders are found on the device once the tables are there (a host pass over the 27 x N
-        # table would cost more than the rest of the construction)
-        on_device = order in ("split", "boundary-first")
+        # the axis and split orders are found on the device once the tables are there (a host pass over the 27 x N
+        # table, or a host sort of the coordinates, would cost more than the rest of the construction)
+        on_device = order in _DEVICE_ORDERS
         perm = None if on_device else node_order(lat, order)
         self.order = order
         self.tau = 3.0 * nu_lu + 0.5
@@ -247,11 +247,7 @@ class Solver:
                 uin = _upload(lat["uin"], torch.float32, dev)
             self.perm = self.inv = None
             if on_device and N:
-                bnd = (nbr < 0).any(0)
-                parts = [torch.nonzero(~bnd).flatten(), torch.nonzero(bnd).flatten()]
-                perm_d = torch.cat(parts[::-1] if order == "boundary-first" else parts)
-                if not bool((perm_d == torch.arange(N, device=dev)).all()):
-                    perm = perm_d
+                perm = _device_order(lat, nbr, order, dev)
             if perm is not None:
                 # internal node k is the lattice's node perm[k]; sources renumbered through inv
                 self.perm = perm if isinstance(perm, torch.Tensor) else torch.as_tensor(perm.astype(np.int64)).to(dev)
@@ -552,6 +548,43 @@ ORDERS = ("c", "axis", "morton", "split", "axis-split", "boundary-first", "axis-
 # orders that separate the nodes with a boundary link from the others, and on which base order
 _SPLITS = {"split": ("c", False), "axis-split": ("axis", False), "boundary-first": ("c", True),
            "axis-boundary-first": ("axis", True)}
+
+
+_DEVICE_ORDERS = ("axis", "split", "axis-split", "boundary-first", "axis-boundary-first")
+
+
+def _device_order(lat, nbr, order, dev):
+    """node_order(lat, order) computed on the device from the (Q, N) table `nbr` already there (and the coordinates,
+    uploaded if the lattice has no device copy): a CUDA int64 tensor, or None for the C order. The same permutation
+    as the host's: the axis order's lexicographic key is one integer per node (coordinates are unique, so the sort
+    has no ties), and the split orders are stable partitions."""
+    N = int(nbr.shape[1])
+    base = None
+    if order.startswith("axis"):
+        tabs = lat.get("_dev") if isinstance(lat.get("_dev"), dict) else {}
+        c = tabs.get("coords")
+        if c is None or c.device != dev:
+            c = torch.as_tensor(np.ascontiguousarray(lat["coords"], np.int32)).to(dev)
+        c = c.to(torch.int64)
+        lo = c.min(0).values
+        ext = c.max(0).values - lo
+        fast = int(torch.argmax(ext).item())              # the first largest extent, as np.argmax
+        s0, s1 = [a for a in (0, 1, 2) if a != fast]
+        span = ext + 1
+        key = ((c[:, s0] - lo[s0]) * span[s1] + (c[:, s1] - lo[s1])) * span[fast] + (c[:, fast] - lo[fast])
+        base = torch.argsort(key)
+    if order == "axis":
+        perm = base
+    else:
+        bnd = (nbr < 0).any(0)
+        if base is not None:
+            bnd = bnd[base]
+        parts = [torch.nonzero(~bnd).flatten(), torch.nonzero(bnd).flatten()]
+        idx = torch.cat(parts[::-1] if _SPLITS[order][1] else parts)
+        perm = idx if base is None else base[idx]
+    if bool((perm == torch.arange(N, device=dev)).all()):
+        return None
+    return perm
 
 
 def node_order(lat, order="c"):

@@ -9,7 +9,7 @@ import torch
 
 pytestmark = pytest.mark.gpu
 
-from cerebrosim_b200 import cases, lbm  # noqa: E402
+from cerebrosim_b200 import cases, lbm, workloads  # noqa: E402
 
 NU = (0.55 - 0.5) / 3.0
 
@@ -53,6 +53,18 @@ def test_split_orders_from_host_tables(pipe, order):
     host = {k: v for k, v in pipe.items() if k != "_dev"}
     s = solver(host, order=order)
     assert np.array_equal(s.perm.cpu().numpy(), lbm.node_order(pipe, order))
+
+
+@pytest.mark.parametrize("order", ["axis", "split", "axis-split", "boundary-first", "axis-boundary-first"])
+def test_device_orders_equal_host_orders(order):
+    """Every order the solver computes on the device is the host's node_order, on a generated artery (whose axis
+    order differs from its C order), from device tables and from host tables (coordinates uploaded)."""
+    lat = workloads.lattice(workloads.stenosed_vessel(3), 0.1)
+    host_perm = lbm.node_order(lat, order)
+    assert host_perm is not None
+    for tables in (lat, {k: v for k, v in lat.items() if k != "_dev"}):
+        s = lbm.Solver(tables, NU, model="regularised", order=order)
+        assert s.perm is not None and np.array_equal(s.perm.cpu().numpy(), host_perm)
 
 
 def test_constructions_reuse_device_memory(pipe):
