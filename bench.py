@@ -280,7 +280,7 @@ def bench_sweep(args, dev, peak, rep):
     updates over the slowest rank's time."""
     import torch
 
-    from cerebrosim_b200 import workloads as W
+    from cerebrosim_b200 import lbm, workloads as W
     from cerebrosim_b200.batch import BatchSolver
 
     from cerebrosim_b200 import autotune
@@ -291,7 +291,7 @@ def bench_sweep(args, dev, peak, rep):
     build_s = time.perf_counter() - t0
     steps = args.sweep_steps
     # block size and node order: tuned on the largest vessel, for its storage format, then used by every member
-    big = max(range(len(specs)), key=lambda k: lats[k]["nbr"].shape[1])
+    big = max(range(len(specs)), key=lambda k: lbm.n_nodes(lats[k]))
     best, table = autotune.tune(lats[big], (0.52 - 0.5) / 3.0, storage=args.sweep_storage, steps=200, warmup=50,
                                 blocks=(128, 256),
                                 configure=lambda s: W.configure(s, specs[big], lats[big]), device=dev,
@@ -312,7 +312,7 @@ def bench_sweep(args, dev, peak, rep):
                        "period 8000 steps)",
            "instances": len(specs), "steps": steps, "build_s": build_s,
            "autotune": {"best": best, "candidates": table, "tuned_on": f"seed {specs[big]['seed']}, "
-                                                                         f"{lats[big]['nbr'].shape[1]} nodes"}}
+                                                                         f"{lbm.n_nodes(lats[big])} nodes"}}
     sol = [W.make_solver(sp, lat, storage=args.sweep_storage, device=dev, block=best["block"], order=best["order"])
            for sp, lat in zip(specs, lats)]
     nodes = sum(x.N for x in sol)

@@ -72,6 +72,8 @@ SIGNATURES = {
     "cs_lattice_count": (_I32, [_P, _I64, _I64, _I64, _P, ctypes.POINTER(_I64), _P]),
     "cs_lattice_fill": (_I32, [_P, _I64, _I64, _I64, ctypes.POINTER(_D), _D, ctypes.POINTER(Opening), _I32, _I32,
                                _D, _P, _I64, _P, _P, _P, _P, _P, _P]),
+    "cs_sponge_om": (_I32, [_P, _I64, ctypes.POINTER(_D), _D, ctypes.POINTER(Opening), _I32, _I32, _D, _D, _D, _P, _P,
+                            _P]),
     "cs_links_scratch_bytes": (_SZ, [_I64]),
     "cs_links_count": (_I32, [_P, _I64, _P, ctypes.POINTER(_I64), _P]),
     "cs_links_fill": (_I32, [_P, _P, _I64, _I32, _I64, _P, _P, _P, _P, _P, _P, _P]),

@@ -31,7 +31,7 @@ def tune(lat, nu_lu, configure=None, storage="f32", blocks=BLOCKS, orders=lbm.OR
     "us_per_step", "mlups"}; table = one such dict per candidate. `configure(solver)` sets the drive, outlets and
     sponge before timing (the boundary work is part of the step)."""
     table = []
-    n = int(lat["nbr"].shape[1])
+    n = lbm.n_nodes(lat)
     seen = set()
     for order in orders:
         perm = lbm.node_order(lat, order)

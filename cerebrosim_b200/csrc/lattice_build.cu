@@ -372,3 +372,82 @@ extern "C" int cs_lattice_fill(const float* phi, int64_t nx, int64_t ny, int64_t
     }
     return CS_OK;
 }
+
+// ---- sponge (lbm.py:398-416) --------------------------------------------------------------------------------------
+// Per-cell relaxation near the openings, in the reference's float64 order of operations and rounding: tau_cell = max
+// over the chosen openings of tau + (tau_max - tau) * smoothstep(clip(1 - depth / length, 0, 1)) where the cell is
+// within 1.5 radii of the opening's axis, depth = -axial / dx; om = float32(1 / tau_cell). The reference's cell
+// positions come from np.argwhere, a column-major (N, 3) array, and NumPy's `rel @ nrm` on it evaluates, on the host
+// that wrote the fixtures, fma(x, n0, y * n1) + z * n2 for all rows but the last N mod 4, and fma(z, n2, fma(y, n1,
+// x * n0)) for those (the column-major BLAS kernel's blocks of four rows and its remainder).
+namespace cs {
+namespace {
+
+struct SpongeSet {
+    int n;
+    double c[MAX_OPENINGS][3];
+    double nrm[MAX_OPENINGS][3];
+    double reach[MAX_OPENINGS];   // 1.5 radius
+};
+
+__global__ void k_sponge(const int32_t* __restrict__ coords, int64_t n, double o0, double o1, double o2, double dx,
+                         SpongeSet ss, double tau, double length, double tau_max, float* __restrict__ om,
+                         double* __restrict__ tau_out) {
+    const int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    if (k >= n) return;
+    const double origin[3] = {o0, o1, o2};
+    double p[3];
+    for (int a = 0; a < 3; ++a) p[a] = __dadd_rn(origin[a], __dmul_rn(double(coords[3 * k + a]), dx));
+    const bool tail = k >= n - n % 4;
+    double out = tau;
+    for (int j = 0; j < ss.n; ++j) {
+        const double* nv = ss.nrm[j];
+        const double r0 = __dsub_rn(p[0], ss.c[j][0]), r1 = __dsub_rn(p[1], ss.c[j][1]);
+        const double r2 = __dsub_rn(p[2], ss.c[j][2]);
+        const double ax = tail ? __fma_rn(r2, nv[2], __fma_rn(r1, nv[1], __dmul_rn(r0, nv[0])))
+                               : __dadd_rn(__fma_rn(r0, nv[0], __dmul_rn(r1, nv[1])), __dmul_rn(r2, nv[2]));
+        const double v0 = __dsub_rn(r0, __dmul_rn(ax, nv[0]));
+        const double v1 = __dsub_rn(r1, __dmul_rn(ax, nv[1]));
+        const double v2 = __dsub_rn(r2, __dmul_rn(ax, nv[2]));
+        const double lat = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(v0, v0), __dmul_rn(v1, v1)), __dmul_rn(v2, v2)));
+        const double depth = __ddiv_rn(-ax, dx);
+        double w = __dsub_rn(1.0, __ddiv_rn(depth, length));
+        w = w < 0.0 ? 0.0 : (w > 1.0 ? 1.0 : w);
+        w = __dmul_rn(__dmul_rn(w, w), __dsub_rn(3.0, __dmul_rn(2.0, w)));
+        const double v = lat < ss.reach[j] ? __dadd_rn(tau, __dmul_rn(__dsub_rn(tau_max, tau), w)) : tau;
+        out = v > out ? v : out;
+    }
+    om[k] = __double2float_rn(__ddiv_rn(1.0, out));
+    if (tau_out) tau_out[k] = out;
+}
+
+}  // namespace
+}  // namespace cs
+
+extern "C" int cs_sponge_om(const int32_t* coords, int64_t n, const double* origin, double dx,
+                            const cs_opening* openings, int32_t n_openings, int32_t kinds_mask, double tau,
+                            double length, double tau_max, float* om, double* tau_out, void* stream) {
+    if (n < 0 || !origin || !(dx > 0.0) || !(length > 0.0) || (kinds_mask & ~3))
+        return fail(CS_ERR_ARG, "cs_sponge_om: bad arguments");
+    if (n_openings < 0 || n_openings > MAX_OPENINGS)
+        return fail(CS_ERR_SIZE, "cs_sponge_om: %d openings (at most %d)", n_openings, MAX_OPENINGS);
+    if (n_openings > 0 && !openings) return fail(CS_ERR_ARG, "cs_sponge_om: null openings");
+    SpongeSet ss{};
+    for (int k = 0; k < n_openings; ++k) {
+        const cs_opening& o = openings[k];
+        if (o.kind != 0 && o.kind != 1) return fail(CS_ERR_ARG, "cs_sponge_om: opening %d kind %d", k, o.kind);
+        if (!(kinds_mask & (1 << o.kind))) continue;
+        const int j = ss.n++;
+        for (int a = 0; a < 3; ++a) {
+            ss.c[j][a] = o.centre[a];
+            ss.nrm[j][a] = o.normal[a];
+        }
+        ss.reach[j] = 1.5 * o.radius;             // one IEEE product, as NumPy
+    }
+    if (n == 0) return CS_OK;
+    if (!coords || !om) return fail(CS_ERR_ARG, "cs_sponge_om: null buffer");
+    k_sponge<<<unsigned(ceil_div(n, 256)), 256, 0, as_stream(stream)>>>(coords, n, origin[0], origin[1], origin[2], dx,
+                                                                      ss, tau, length, tau_max, om, tau_out);
+    CS_CHECK_LAUNCH("k_sponge");
+    return CS_OK;
+}

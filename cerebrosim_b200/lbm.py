@@ -76,12 +76,35 @@ def ctypes_void(x):
     return ctypes.c_void_p(int(x))
 
 
-def build_lattice(phi, origin, dx, openings=(), periodic=(), opening_slack=1.0, device=None):
+class Lattice(dict):
+    """build_lattice's result: the reference's dict. When built with host=False its host tables (nbr, q, uin,
+    coords) are copied from the device copies in "_dev" the first time they are read, so a caller that only hands
+    the lattice to a Solver (which uses the device copies) never moves them."""
+
+    _LAZY = ("nbr", "q", "uin", "coords")
+
+    def __missing__(self, key):
+        dev = dict.get(self, "_dev")
+        if key in self._LAZY and isinstance(dev, dict) and key in dev:
+            v = dev[key].cpu().numpy()
+            self[key] = v
+            return v
+        raise KeyError(key)
+
+
+def n_nodes(lat):
+    """Fluid node count of a lattice, without reading its host tables."""
+    dev = lat.get("_dev") if isinstance(lat.get("_dev"), dict) else None
+    return int((dev if dev is not None else lat)["nbr"].shape[1])
+
+
+def build_lattice(phi, origin, dx, openings=(), periodic=(), opening_slack=1.0, device=None, host=True):
     """Sparse lattice from a signed distance on grid nodes (negative = fluid), built on the GPU (lbm.py:264-330).
 
     Returns the reference's dict of NumPy arrays (nbr (Q, N) int32, q (Q, N) float32, uin (N, 3) float32,
     coords (N, 3) int32, origin, dx, shape, n_outlets, counts, openings), bit-identical to lbm.build_lattice, plus
-    "_dev": the same tables as CUDA tensors, which `Solver` reuses instead of uploading them again."""
+    "_dev": the same tables as CUDA tensors, which `Solver` reuses instead of uploading them again. host=False: the
+    four host tables are copied from "_dev" only when first read (`Lattice`)."""
     lib = _lib.load()
     if isinstance(phi, torch.Tensor) and phi.is_cuda:   # a field already on the device (vessel.sdf_grid)
         dev = _device(phi.device if device is None else device)
@@ -138,10 +161,13 @@ def build_lattice(phi, origin, dx, openings=(), periodic=(), opening_slack=1.0, 
         stream.synchronize()
         del scratch, phi_d
     cnt = counts.cpu().numpy()
-    return {"nbr": nbr.cpu().numpy(), "q": q.cpu().numpy(), "uin": uin.cpu().numpy(), "coords": coords.cpu().numpy(),
-            "origin": origin_a, "dx": dx, "shape": shape, "n_outlets": len(outlets),
-            "counts": {"wall": int(cnt[0]), "inlet": int(cnt[1]), "outlet": [int(x) for x in cnt[2:]]},
-            "openings": inlets + outlets, "_dev": {"nbr": nbr, "q": q, "uin": uin, "coords": coords}}
+    lat = Lattice(origin=origin_a, dx=dx, shape=shape, n_outlets=len(outlets),
+                  counts={"wall": int(cnt[0]), "inlet": int(cnt[1]), "outlet": [int(x) for x in cnt[2:]]},
+                  openings=inlets + outlets, _dev={"nbr": nbr, "q": q, "uin": uin, "coords": coords})
+    if host:
+        for k in Lattice._LAZY:
+            lat[k]
+    return lat
 
 
 def scatter(lat, values, fill=np.nan):
@@ -199,7 +225,7 @@ class Solver:
         lib = _lib.load()
         self.dev = _device(device)
         self.lat = lat
-        self.N = N = int(lat["nbr"].shape[1])
+        self.N = N = n_nodes(lat)
         # the axis and split orders are found on the device once the tables are there (a host pass over the 27 x N
         # table, or a host sort of the coordinates, would cost more than the rest of the construction)
         on_device = order in _DEVICE_ORDERS
@@ -337,14 +363,54 @@ class Solver:
         self._drop_graphs()
 
     def set_sponge(self, length, tau_max, kinds=("inlet", "outlet")):
-        """Raise the viscosity smoothly towards the openings of the given kinds (lbm.py:398-416)."""
-        tau = sponge_tau(self.lat, self.tau, length, tau_max, kinds)
-        self.tau_cell = tau
-        with torch.cuda.device(self.dev), torch.cuda.stream(self.stream):
-            om = torch.as_tensor((1.0 / tau).astype(np.float32)).to(self.dev)
+        """Raise the viscosity smoothly towards the openings of the given kinds (lbm.py:398-416). Computed on the
+        device (csrc/lattice_build.cu k_sponge) with the reference's float64 operations: the same per-cell tau as
+        `sponge_tau`, which restates it on the host."""
+        mask = (1 if "inlet" in kinds else 0) | (2 if "outlet" in kinds else 0)
+        ops = list(self.lat["openings"])
+        carr = (_lib.Opening * max(1, len(ops)))()
+        for j, o in enumerate(ops):
+            carr[j].kind = 0 if o["kind"] == "inlet" else 1
+            c, nrm = np.asarray(o["centre"], float), np.asarray(o["normal"], float)
+            for a in range(3):
+                carr[j].centre[a] = float(c[a])
+                carr[j].normal[a] = float(nrm[a])
+            carr[j].radius = float(o["radius"])
+        self._sponge = (carr, len(ops), mask, float(length), float(tau_max))
+        with torch.cuda.device(self.dev):
+            # on the caller's stream (temporaries from its pool), after the steps already enqueued
+            cur = torch.cuda.current_stream(self.dev)
+            cur.wait_stream(self.stream)
+            om = self._sponge_eval(cur)
             if self.perm is not None:
                 om = om[self.perm]
             self.om.copy_(om * self._om_sign)
+            self.stream.wait_stream(cur)
+
+    def _sponge_eval(self, stream, tau_out=None):
+        """om = float32(1 / tau_cell) per cell (lattice order) of the last set_sponge, on `stream`."""
+        carr, n_ops, mask, length, tau_max = self._sponge
+        org = (ctypes.c_double * 3)(*np.asarray(self.lat["origin"], float).reshape(3).tolist())
+        tabs = self.lat.get("_dev") if isinstance(self.lat.get("_dev"), dict) else {}
+        coords = tabs.get("coords")
+        if coords is None or coords.device != self.dev:
+            coords = torch.as_tensor(np.ascontiguousarray(self.lat["coords"], np.int32)).to(self.dev)
+        om = torch.empty(self.N, dtype=torch.float32, device=self.dev)
+        check(_lib.load().cs_sponge_om(_ptr(coords), self.N, org, float(self.lat["dx"]), carr, n_ops, mask,
+                                       float(self.tau), length, tau_max, _ptr(om), _ptr(tau_out),
+                                       ctypes_void(stream.cuda_stream)))
+        return om
+
+    @property
+    def tau_cell(self):
+        """Relaxation time per cell (lattice order, float64 NumPy; lbm.py:366, 415), evaluated on request."""
+        if getattr(self, "_sponge", None) is None:
+            return np.full(self.N, self.tau)
+        with torch.cuda.device(self.dev):
+            cur = torch.cuda.current_stream(self.dev)
+            tau = torch.empty(self.N, dtype=torch.float64, device=self.dev)
+            self._sponge_eval(cur, tau)
+            return tau.cpu().numpy()
 
     def set_outlet_pressure(self, p_lu):
         p = np.asarray(p_lu, np.float32).reshape(-1)

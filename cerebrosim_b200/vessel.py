@@ -129,9 +129,10 @@ def openings_of(g):
     return ops
 
 
-def artery_lattice(g, dx_mm, openings=None, lo=None, hi=None, device=None):
+def artery_lattice(g, dx_mm, openings=None, lo=None, hi=None, device=None, host=True):
     """validate.py:294-308: the vessel's lattice at dx_mm, field and tables built on the device.
-    `g` is a geometry dict, or a `Packed` with explicit `openings`, `lo` and `hi`."""
+    `g` is a geometry dict, or a `Packed` with explicit `openings`, `lo` and `hi`; host=False: host tables copied
+    only when read (lbm.Lattice)."""
     if isinstance(g, Packed):
         if openings is None or lo is None:
             raise ValueError("a packed vessel needs its openings and bounds")
@@ -139,7 +140,7 @@ def artery_lattice(g, dx_mm, openings=None, lo=None, hi=None, device=None):
         openings = openings_of(g) if openings is None else openings
     phi, origin = sdf_grid(g, dx_mm, lo, hi, device=device, host=False)
     ops = sorted(openings, key=lambda o: o["kind"] != "inlet")
-    lat = lbm.build_lattice(phi, origin, dx_mm, openings=ops, device=phi.device)
+    lat = lbm.build_lattice(phi, origin, dx_mm, openings=ops, device=phi.device, host=host)
     del phi
     lat["openings"] = ops
     return lat

@@ -106,8 +106,9 @@ def openings(g):
 
 
 def lattice(g, dx, device=None):
-    """The vessel's lattice at dx mm, voxelised and built on the GPU."""
-    return vessel.artery_lattice(g, dx, openings=openings(g), device=device)
+    """The vessel's lattice at dx mm, voxelised and built on the GPU; its host tables are copied from the device
+    only when read (a solver uses the device copies)."""
+    return vessel.artery_lattice(g, dx, openings=openings(g), device=device, host=False)
 
 
 def fourier_drive(seed, mean=0.03, peak_over_mean=1.8, harmonics=4, floor=0.2):

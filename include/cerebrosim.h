@@ -96,6 +96,16 @@ int cs_lattice_fill(const float* phi, int64_t nx, int64_t ny, int64_t nz, const 
                     void* scratch, int64_t n_fluid, int32_t* nbr, float* q, float* uin, int32_t* coords,
                     int64_t* counts, void* stream);
 
+/* Sponge (replaces Solver.set_sponge's host computation, lbm.py:398-416) for the n nodes of `coords` (device, N*3
+ * int32): per node tau_cell = max over the openings whose kind bit is set in kinds_mask (bit 0 inlets, bit 1
+ * outlets) of tau + (tau_max - tau) * smoothstep(clip(1 - depth / length, 0, 1)) within 1.5 radii of the opening's
+ * axis (depth = inward distance from the opening plane in cells), in the reference's float64 operations and
+ * rounding. Outputs (device): om[n] = float32(1 / tau_cell); tau_out[n] = tau_cell (float64), or null.
+ * openings: HOST array. */
+int cs_sponge_om(const int32_t* coords, int64_t n, const double* origin, double dx, const cs_opening* openings,
+                 int32_t n_openings, int32_t kinds_mask, double tau, double length, double tau_max, float* om,
+                 double* tau_out, void* stream);
+
 /* ---------------------------------------------------------------------------------------------------------------
  * Step — replaces lbm.k_clock + lbm.k_step (lbm.py:90-257) and, when n_open > 0, simulate.k_flux + simulate.k_bc
  * (simulate.py:65-82).

@@ -62,7 +62,8 @@ def test_device_orders_equal_host_orders(order):
     lat = workloads.lattice(workloads.stenosed_vessel(3), 0.1)
     host_perm = lbm.node_order(lat, order)
     assert host_perm is not None
-    for tables in (lat, {k: v for k, v in lat.items() if k != "_dev"}):
+    host = {k: lat[k] for k in list(lat) + ["nbr", "q", "uin", "coords"] if k != "_dev"}   # host copies read
+    for tables in (lat, host):
         s = lbm.Solver(tables, NU, model="regularised", order=order)
         assert s.perm is not None and np.array_equal(s.perm.cpu().numpy(), host_perm)
 
@@ -104,3 +105,29 @@ def test_pinned_host_tables(pipe, order):
     pa, ua = a.fields()
     pb, ub = b.fields()
     assert np.array_equal(pa, pb) and np.array_equal(ua, ub)
+
+
+def test_lazy_host_tables():
+    """A workload lattice (host=False) copies its host tables from the device only when read; what it then holds is
+    the eager build's, bit for bit, and a solver built before any read equals one built after."""
+    g = workloads.stenosed_vessel(3)
+    lazy = workloads.lattice(g, 0.1)
+    assert not any(k in dict.keys(lazy) for k in ("nbr", "q", "uin", "coords"))
+    s0 = lbm.Solver(lazy, NU, model="regularised", order="axis-boundary-first")
+    assert not any(k in dict.keys(lazy) for k in ("nbr", "q", "uin", "coords"))    # the solver read none of them
+    eager = lbm.build_lattice(*_field(g, 0.1), openings=workloads.openings(g))
+    for k in ("nbr", "q", "uin", "coords"):
+        assert np.array_equal(lazy[k], eager[k]), k
+    s1 = lbm.Solver(eager, NU, model="regularised", order="axis-boundary-first")
+    for s in (s0, s1):
+        workloads.configure(s, {"seed": 3, "stenosis": 0.7, "pressure": 95.0}, eager)
+        s.run(50)
+    p0, u0 = s0.fields()
+    p1, u1 = s1.fields()
+    assert np.array_equal(p0, p1) and np.array_equal(u0, u1)
+
+
+def _field(g, dx):
+    from cerebrosim_b200 import vessel
+    phi, origin = vessel.sdf_grid(g, dx, host=False)
+    return phi, origin, dx

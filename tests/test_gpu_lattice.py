@@ -112,3 +112,23 @@ def test_builder_limits():
         lbm.build_lattice(phi, [0, 0, 0], 1.0, periodic=(3,))
     with pytest.raises(ValueError):
         lbm.build_lattice(phi[0], [0, 0, 0], 1.0)
+
+
+def test_sponge_on_the_device_equals_the_reference(golden):
+    """Solver.set_sponge evaluates the sponge on the device (k_sponge): per-cell tau and the float32 1 / tau equal
+    the reference's own set_sponge output (tests/golden/sponge.npz) bit for bit, for inlet and outlet sponges of
+    several lengths; C order and a renumbered order give the same cells."""
+    import json
+    meta, arr = golden.small_case("open_pipe_tilted_R4")
+    lat = lbm.build_lattice(arr["phi"], meta["origin"], meta["dx"], openings=meta["openings"])
+    for order in ("c", "boundary-first"):
+        for tag in ("a", "b", "c"):
+            args = json.loads(str(golden.sponge[f"{tag}/args"]))
+            s = lbm.Solver(lat, 0.02, model="regularised", order=order)
+            s.tau = args["tau"]                       # the reference's tau itself, not 3 nu + 0.5 recomputed
+            s.set_sponge(args["length"], args["tau_max"], tuple(args["kinds"]))
+            assert np.array_equal(s.tau_cell, golden.sponge[f"{tag}/tau_cell"]), tag
+            om = s.om.abs()
+            if s.inv is not None:
+                om = om[s.inv]
+            assert np.array_equal(om.cpu().numpy(), golden.sponge[f"{tag}/om"]), tag
