@@ -1,5 +1,6 @@
 """The synthetic workloads: generated vessels, inflow waveform, sweep and request stream (host side)."""
 import numpy as np
+import pytest
 
 from cerebrosim_b200 import vessel, workloads as W
 from oracle import sdf_ref
@@ -124,3 +125,21 @@ def test_boundary_first_order_puts_boundary_nodes_first():
     axis = np.arange(len(bnd)) if axis is None else axis              # None: the axis order is the C order
     perm = lbm.node_order(lat, "axis-boundary-first")
     assert np.array_equal(perm, np.concatenate([axis[bnd[axis]], axis[~bnd[axis]]]))
+
+
+def test_lattice_host_tables_are_copied_on_first_read():
+    """lbm.Lattice (build_lattice(..., host=False)): a host table missing from the dict is copied from its device copy
+    the first time it is read and then kept; other missing keys raise KeyError; n_nodes reads no host table."""
+    import torch
+    from cerebrosim_b200 import lbm
+    nbr = torch.arange(27 * 5, dtype=torch.int32).reshape(27, 5)
+    dev = {"nbr": nbr, "q": nbr.float(), "uin": torch.zeros(5, 3), "coords": torch.zeros(5, 3)}
+    lat = lbm.Lattice(dx=1.0, _dev=dev)
+    assert lbm.n_nodes(lat) == 5 and "nbr" not in dict.keys(lat)
+    got = lat["nbr"]
+    assert isinstance(got, np.ndarray) and np.array_equal(got, nbr.numpy()) and "nbr" in dict.keys(lat)
+    assert lat["nbr"] is got
+    assert "q" not in dict.keys(lat)
+    with pytest.raises(KeyError):
+        lat["nothing"]
+    assert lbm.n_nodes({"nbr": np.zeros((27, 7), np.int32)}) == 7
