@@ -143,3 +143,22 @@ def test_lattice_host_tables_are_copied_on_first_read():
     with pytest.raises(KeyError):
         lat["nothing"]
     assert lbm.n_nodes({"nbr": np.zeros((27, 7), np.int32)}) == 7
+
+
+def test_device_node_orders_equal_host_orders_on_cpu_tensors():
+    """The solver's device computation of the axis and split orders (lbm._device_order: an argsort of one integer key
+    per node, stable partitions by the boundary mask) gives node_order's permutations; run here on CPU tensors, on a
+    pipe along x (its longest axis is not the C order's fastest) with an inlet and an outlet."""
+    import torch
+    from cerebrosim_b200 import lbm
+    from oracle import lattice_ref as L
+    x, y, z = np.meshgrid(np.arange(60), np.arange(14), np.arange(16), indexing="ij")
+    phi = (np.sqrt((y - 6.5) ** 2 + (z - 7.2) ** 2) - 5.0).astype(np.float32)
+    ops = [{"kind": "inlet", "centre": [0.5, 6.5, 7.2], "normal": [1, 0, 0], "radius": 6.0},
+           {"kind": "outlet", "centre": [58.5, 6.5, 7.2], "normal": [-1, 0, 0], "radius": 6.0}]
+    lat = L.build_lattice(phi, [0, 0, 0], 1.0, openings=ops)
+    nbr = torch.as_tensor(lat["nbr"])
+    for order in lbm._DEVICE_ORDERS:
+        host = lbm.node_order(lat, order)
+        dev = lbm._device_order(lat, nbr, order, torch.device("cpu"))
+        assert host is not None and dev is not None and np.array_equal(dev.numpy(), host), order
