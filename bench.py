@@ -536,7 +536,13 @@ def main():
         t_host.append(time.perf_counter())
         parts = {"construct": (t_host[1] - t_host[0]) * 1e3, "run": (t_host[2] - t_host[1]) * 1e3,
                  "fields": (t_host[3] - t_host[2]) * 1e3}
-        return e0.elapsed_time(e1) * 1e-3, parts, p_h.nbytes + u_h.nbytes
+        secs = e0.elapsed_time(e1) * 1e-3
+        # release this run's solver and its CUDA graphs here, after its timed region, so that their teardown does
+        # not land in the next run's construction
+        s2._drop_graphs()
+        del s2
+        torch.cuda.synchronize()
+        return secs, parts, p_h.nbytes + u_h.nbytes
 
     # three end-to-end runs (each: construction from the host tables, the K steps, the read-back); the median is
     # reported, so that one run disturbed by the host (a construction of 23 ms instead of 4 was seen) does not
