@@ -24,6 +24,7 @@ At N = 1 the line also carries
   over the makespan; beside it the same requests one by one in plain FP32, builds included in both.
 """
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -542,6 +543,7 @@ def main():
         s2._drop_graphs()
         del s2
         torch.cuda.synchronize()
+        gc.collect()                  # and collect the host's garbage between runs, not inside the next one
         return secs, parts, p_h.nbytes + u_h.nbytes
 
     # three end-to-end runs (each: construction from the host tables, the K steps, the read-back); the median is
